@@ -1,0 +1,189 @@
+/*
+ * llg_b200.h — C ABI of the B200 (sm_100a) implementation of llg-sim's
+ * uniform-grid LLG hot path.
+ *
+ * Scope: effective field (exchange, uniaxial anisotropy, interfacial DMI,
+ * Zeeman, zero-padded FFT demag), the LLG torque, the Dormand–Prince RK45
+ * and Bogacki–Shampine RK23 relax steppers, the relax controller and the
+ * energy bookkeeping.  Each entry point names the llg-sim (Rust) interface it
+ * replaces, as file:line in that project.
+ *
+ * Conventions
+ *  - Host arrays use the reference layout: AoS double[3] per cell, cell index
+ *    j*nx + i (grid.rs:27-30, vector_field.rs:24-27).  Masks are one byte per
+ *    cell, nonzero = material.
+ *  - Every call returns an int status: LLG_OK (0) or a negative LLG_ERR_*.
+ *    No exception or abort crosses the ABI; llg_last_error() returns the
+ *    message of the calling thread's last failure.
+ *  - The caller owns every host array; the library copies in and out.  Device
+ *    buffers are owned by the handle that allocated them.
+ *  - A handle is not thread-safe; distinct handles are.  Each solver / batch
+ *    issues its work on one CUDA stream (llg_*_set_stream may replace it).
+ *  - Precision: LLG_PREC_FP32 runs fields, FFTs and stages in FP32 with FP64
+ *    kernel construction, error norms, step controllers and convergence
+ *    reductions; LLG_PREC_FP64 runs everything in FP64.
+ */
+#ifndef LLG_B200_H
+#define LLG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LLG_B200_ABI_VERSION 1
+
+enum llg_status {
+    LLG_OK = 0,
+    LLG_ERR_INVALID = -1,   /* bad argument / unsupported size */
+    LLG_ERR_CUDA = -2,      /* CUDA runtime error */
+    LLG_ERR_TIMEOUT = -3,   /* a bounded device wait gave up */
+    LLG_ERR_NONFINITE = -4, /* NaN/Inf in the state or the error norm; the film is retired */
+    LLG_ERR_OOM = -5,       /* device allocation failed */
+    LLG_ERR_NO_DEVICE = -6  /* no usable sm_100 device */
+};
+
+/* FieldMask, effective_field/mod.rs:38-45 */
+enum llg_field_mask { LLG_FIELD_EXCH_ANIS = 0, LLG_FIELD_EXCH_ANIS_DMI = 1, LLG_FIELD_FULL = 2 };
+/* TorqueMetric, relax.rs:32-37 */
+enum llg_torque_metric { LLG_TORQUE_MAX = 0, LLG_TORQUE_MEAN = 1, LLG_TORQUE_RMS = 2, LLG_TORQUE_MEANSQ = 3 };
+enum llg_precision { LLG_PREC_FP32 = 0, LLG_PREC_FP64 = 1 };
+
+/* Grid2D, grid.rs:4-11 */
+typedef struct llg_grid {
+    int64_t nx, ny;
+    double dx, dy, dz;
+} llg_grid;
+
+/* Material, params.rs:170-184 (demag_method: only the FFT method is on this path) */
+typedef struct llg_material {
+    double ms, a_ex, k_u;
+    double easy_axis[3];
+    double dmi;      /* J/m^2, used when has_dmi != 0 (Option<f64>) */
+    int32_t has_dmi;
+    int32_t demag;   /* Material::demag */
+} llg_material;
+
+/* LLGParams, params.rs:213-219 */
+typedef struct llg_params {
+    double gamma, alpha, dt;
+    double b_ext[3];
+} llg_params;
+
+/* RelaxSettings, relax.rs:73-105 (Option<f64> fields as has_* + value) */
+typedef struct llg_relax_settings {
+    double max_err, headroom, dt_min, dt_max;
+    int32_t phase1_enabled, phase2_enabled;
+    int64_t energy_stride;
+    double rel_energy_tol;
+    int32_t torque_metric;
+    int32_t has_torque_threshold;
+    double torque_threshold;
+    int64_t torque_check_stride;
+    double torque_plateau_rel, torque_plateau_abs;
+    int64_t torque_plateau_checks, torque_plateau_min_checks;
+    double tighten_factor, tighten_floor;
+    int64_t max_accepted_steps;
+    int32_t has_final_torque_gate, has_final_torque_gate_max;
+    double final_torque_gate, final_torque_gate_max;
+    int64_t gate_max_extra_accepted_steps, gate_plateau_fails;
+} llg_relax_settings;
+
+/* RelaxReport, relax.rs:55-71; stop_reason in RelaxStopReason order
+ * (relax.rs:40-45), last_stage_stop -1 = None else RelaxStageStop order (relax.rs:48-52) */
+typedef struct llg_relax_report {
+    int64_t accepted_steps, rejected_steps, torque_checks, torque_field_rebuilds;
+    int32_t stop_reason;
+    int32_t last_stage_stop;
+    int32_t has_final_torque, has_final_torque_max;
+    double final_torque, final_torque_max, final_max_err, final_dt;
+} llg_relax_report;
+
+/* EnergyBreakdown, energy.rs:22-28 (Joule) */
+typedef struct llg_energy_breakdown {
+    double exchange, anisotropy, zeeman, dmi, demag;
+} llg_energy_breakdown;
+
+typedef struct llg_ctx llg_ctx;
+typedef struct llg_solver llg_solver;
+
+/* ---------------- context ---------------- */
+int llg_ctx_create(int device, llg_ctx** out);
+int llg_ctx_destroy(llg_ctx* ctx);
+/* Message of the calling thread's last failure (always NUL-terminated). */
+int llg_last_error(char* buf, size_t len);
+int llg_abi_version(void);
+
+/* ---------------- single film ----------------
+ * llg_solver_create builds the demag operator for the grid (the role of
+ * get_demag_operator / Demag2D::new, demag_fft_uniform.rs:86-108, 470-634):
+ * FP64 face-charge kernel integration and FP64 FFT on the GPU, stored as four
+ * real Fourier planes (xx, xy, yy, zz) in the solver precision.
+ * geom_mask (nullable) switches on the geometry-aware path (field per
+ * build_h_eff_masked_geom, mod.rs:78-101; energy per compute_energy_geom,
+ * energy.rs:80-285; vacuum cells pinned at m = 0 through the steppers). */
+int llg_solver_create(llg_ctx* ctx, const llg_grid* grid, const llg_material* mat, int32_t precision,
+                      const uint8_t* geom_mask, llg_solver** out);
+int llg_solver_destroy(llg_solver* s);
+/* Use an external CUDA stream (cudaStream_t passed as void*; NULL = own stream). */
+int llg_solver_set_stream(llg_solver* s, void* stream);
+int llg_solver_sync(llg_solver* s);
+
+/* Upload / download the resident magnetisation (VectorField2D::data). */
+int llg_set_state(llg_solver* s, const double* m_aos);
+int llg_get_state(llg_solver* s, double* m_aos);
+/* Mean magnetisation <m> of the resident state, FP64 reduction on the GPU. */
+int llg_mean_m(llg_solver* s, double out3[3]);
+
+/* build_h_eff_masked (effective_field/mod.rs:48-75; _geom variant mod.rs:78-101)
+ * evaluated at the resident state; b_out: AoS double[3] per cell (Tesla). */
+int llg_build_h_eff(llg_solver* s, const llg_params* params, int32_t field_mask, double* b_out);
+/* demag::compute_demag_field (demag.rs:57-64 -> demag_fft_uniform.rs:146-186) at the resident state. */
+int llg_compute_demag_field(llg_solver* s, double* b_out);
+
+/* step_llg_rk45_recompute_field_masked_adaptive (llg.rs:795-1026): one attempt
+ * on the resident state.  params->dt is read as dt0 and overwritten with the
+ * next step size, as the reference mutates LLGParams::dt.  FSAL reuse follows
+ * llg.rs:854-867 (valid after an accepted step with the same mask and b_ext). */
+int llg_step_rk45(llg_solver* s, llg_params* params, int32_t field_mask, double max_err, double headroom,
+                  double dt_min, double dt_max, double* eps, int32_t* accepted, double* dt_used);
+/* step_llg_rk23_recompute_field_masked_relax_adaptive (llg.rs:278-436). */
+int llg_step_rk23_relax(llg_solver* s, llg_params* params, int32_t field_mask, double max_err, double headroom,
+                        double dt_min, double dt_max, double* eps, int32_t* accepted, double* dt_used);
+
+/* Device-resident RK45 integration: repeats attempts on the GPU without host
+ * round trips until `n_accepted` more steps are accepted or the simulated time
+ * reaches t_end (dt is clamped to land on t_end, as the drivers do in
+ * st_problems/sp4.rs:308-314).  Pass n_accepted < 0 or t_end = +inf to disable
+ * either limit.  max_attempts bounds the work. */
+int llg_run_rk45(llg_solver* s, llg_params* params, int32_t field_mask, double max_err, double headroom,
+                 double dt_min, double dt_max, int64_t n_accepted, double t_end, int64_t max_attempts,
+                 int64_t* accepted_out, int64_t* rejected_out, double* t_advanced);
+
+/* relax_with_report (relax.rs:334-768).  settings->max_err is written back. */
+int llg_relax(llg_solver* s, llg_params* params, int32_t field_mask, llg_relax_settings* settings,
+              llg_relax_report* report);
+void llg_default_relax_settings(llg_relax_settings* st); /* impl Default, relax.rs:107-141 */
+
+/* compute_energy / compute_energy_geom (energy.rs:66-285) at the resident state. */
+int llg_compute_energy(llg_solver* s, const double b_ext[3], llg_energy_breakdown* out);
+/* torque_metric_rebuild (relax.rs:192-203): field rebuild + metric, FP64 reduction. */
+int llg_torque_metric(llg_solver* s, const llg_params* params, int32_t field_mask, int32_t metric,
+                      double* out);
+
+/* Demag operator export: the four real Fourier planes (xx, xy, yy, zz) of
+ * K = mu0 * N on kx in [0,nx], ky in [0,ny], as FP64, without the 1/(px*py)
+ * scaling (compare with the real part of Demag2D::kxx.. at those indices). */
+int llg_demag_kernel_kspace(llg_solver* s, double* out /* 4*(nx+1)*(ny+1) */);
+
+/* ---------------- initial states (initial_states.rs) ---------------- */
+void llg_init_random(int64_t n, uint64_t seed, double* m_aos);                   /* :59-68 */
+void llg_init_uniform_with_noise(int64_t n, const double dir[3], double noise,  /* :43-56 */
+                                 uint64_t seed, double* m_aos);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LLG_B200_H */

@@ -1,0 +1,40 @@
+// build_api.h — host-side entry points shared between the compilation units.
+#pragma once
+#include <cuda_runtime.h>
+#include "types.cuh"
+
+namespace llg {
+
+FftPlan make_plan(int L);
+cudaError_t launch_twiddles(void* tw, int L2, bool fp64, cudaStream_t s);
+template <typename R>
+cudaError_t launch_fft_strided(void* data, int L, const void* tw2, long long elem_stride, int nsig_a,
+                               long long stride_a, int nsig_b, long long stride_b, bool inverse, cudaStream_t s);
+
+// Builds the demag kernel spectrum of an open-boundary nx x ny grid in FP64 on
+// the GPU.  khat_out: (nx+1)*(ny+1) real4 in the solver precision, scaled by
+// 1/(4 nx ny); k64_out_dev: 4*(ny+1)*(nx+1) doubles, unscaled, layout [c][ky][kx].
+// Synchronises the stream.
+cudaError_t build_demag_kernel(int nx, int ny, double dx, double dy, double dz, bool fp64_out, void* khat_out,
+                               double* k64_out_dev, cudaStream_t s);
+
+// Launch geometry of one film set.
+struct LaunchGeom {
+    const FilmDev* films;
+    const WorkItem* row_items;
+    int n_row_items;
+    const WorkItem* col_items;
+    int n_col_items;
+    size_t smem_row;
+    size_t smem_col;
+    int grid_row;
+    int grid_col;
+    bool any_demag;
+};
+
+template <typename R>
+cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s);
+template <typename R>
+cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col);
+
+}  // namespace llg

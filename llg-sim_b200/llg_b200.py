@@ -1,0 +1,352 @@
+"""Python host mirror of llg-sim's uniform-grid API over the C ABI of libllg_b200.so.
+
+The names follow the reference's Rust API (Grid2D, Material, LLGParams,
+FieldMask, RelaxSettings, build_h_eff_masked, step_llg_rk45_..._adaptive,
+step_llg_rk23_..._relax_adaptive, relax_with_report, compute_energy) so that
+code written against the reference reads the same.  Every call goes through
+the C ABI declared in include/llg_b200.h; there is no CPU fallback: loading
+fails loudly when the CUDA library has not been built.
+
+Arrays are numpy float64 in the reference layout: AoS ``[nx*ny, 3]`` with cell
+index ``j*nx + i`` (grid.rs:27-30, vector_field.rs:24-27).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libllg_b200.so")
+
+# FieldMask (effective_field/mod.rs:38-45)
+EXCH_ANIS, EXCH_ANIS_DMI, FULL = 0, 1, 2
+# TorqueMetric (relax.rs:32-37)
+TORQUE_MAX, TORQUE_MEAN, TORQUE_RMS, TORQUE_MEANSQ = 0, 1, 2, 3
+FP32, FP64 = 0, 1
+MU0 = 4.0 * np.pi * 1e-7                  # params.rs:15
+GAMMA_E_RAD_PER_S_T = 1.76085963023e11     # params.rs:16
+
+ERRORS = {-1: "LLG_ERR_INVALID", -2: "LLG_ERR_CUDA", -3: "LLG_ERR_TIMEOUT", -4: "LLG_ERR_NONFINITE",
+          -5: "LLG_ERR_OOM", -6: "LLG_ERR_NO_DEVICE"}
+
+
+class LLGError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Grid(C.Structure):
+    _fields_ = [("nx", C.c_int64), ("ny", C.c_int64), ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double)]
+
+
+class _Material(C.Structure):
+    _fields_ = [("ms", C.c_double), ("a_ex", C.c_double), ("k_u", C.c_double), ("easy_axis", C.c_double * 3),
+                ("dmi", C.c_double), ("has_dmi", C.c_int32), ("demag", C.c_int32)]
+
+
+class _Params(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("alpha", C.c_double), ("dt", C.c_double), ("b_ext", C.c_double * 3)]
+
+
+class RelaxSettings(C.Structure):
+    """RelaxSettings (relax.rs:73-105); defaults from impl Default (relax.rs:107-141)."""
+    _fields_ = [("max_err", C.c_double), ("headroom", C.c_double), ("dt_min", C.c_double), ("dt_max", C.c_double),
+                ("phase1_enabled", C.c_int32), ("phase2_enabled", C.c_int32), ("energy_stride", C.c_int64),
+                ("rel_energy_tol", C.c_double), ("torque_metric", C.c_int32), ("has_torque_threshold", C.c_int32),
+                ("torque_threshold", C.c_double), ("torque_check_stride", C.c_int64),
+                ("torque_plateau_rel", C.c_double), ("torque_plateau_abs", C.c_double),
+                ("torque_plateau_checks", C.c_int64), ("torque_plateau_min_checks", C.c_int64),
+                ("tighten_factor", C.c_double), ("tighten_floor", C.c_double), ("max_accepted_steps", C.c_int64),
+                ("has_final_torque_gate", C.c_int32), ("has_final_torque_gate_max", C.c_int32),
+                ("final_torque_gate", C.c_double), ("final_torque_gate_max", C.c_double),
+                ("gate_max_extra_accepted_steps", C.c_int64), ("gate_plateau_fails", C.c_int64)]
+
+    @classmethod
+    def default(cls, **kw):
+        s = cls()
+        lib().llg_default_relax_settings(C.byref(s))
+        for k, v in kw.items():
+            if k == "torque_threshold":
+                s.has_torque_threshold = 0 if v is None else 1
+                s.torque_threshold = 0.0 if v is None else float(v)
+            else:
+                setattr(s, k, v)
+        return s
+
+
+class RelaxReport(C.Structure):
+    _fields_ = [("accepted_steps", C.c_int64), ("rejected_steps", C.c_int64), ("torque_checks", C.c_int64),
+                ("torque_field_rebuilds", C.c_int64), ("stop_reason", C.c_int32), ("last_stage_stop", C.c_int32),
+                ("has_final_torque", C.c_int32), ("has_final_torque_max", C.c_int32),
+                ("final_torque", C.c_double), ("final_torque_max", C.c_double),
+                ("final_max_err", C.c_double), ("final_dt", C.c_double)]
+
+
+class EnergyBreakdown(C.Structure):
+    _fields_ = [("exchange", C.c_double), ("anisotropy", C.c_double), ("zeeman", C.c_double),
+                ("dmi", C.c_double), ("demag", C.c_double)]
+
+    def total(self):
+        return self.exchange + self.anisotropy + self.zeeman + self.dmi + self.demag
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    """The loaded C ABI.  Raises if the CUDA library is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `make -C {_HERE}` (no CPU fallback exists)")
+        L = C.CDLL(LIB_PATH)
+        vp, dp, i32, i64 = C.c_void_p, C.POINTER(C.c_double), C.c_int32, C.c_int64
+        P = C.POINTER
+        sig = {
+            "llg_abi_version": (C.c_int, []),
+            "llg_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+            "llg_ctx_create": (C.c_int, [C.c_int, P(vp)]),
+            "llg_ctx_destroy": (C.c_int, [vp]),
+            "llg_solver_create": (C.c_int, [vp, P(_Grid), P(_Material), i32, vp, P(vp)]),
+            "llg_solver_destroy": (C.c_int, [vp]),
+            "llg_solver_set_stream": (C.c_int, [vp, vp]),
+            "llg_solver_sync": (C.c_int, [vp]),
+            "llg_set_state": (C.c_int, [vp, dp]),
+            "llg_get_state": (C.c_int, [vp, dp]),
+            "llg_mean_m": (C.c_int, [vp, dp]),
+            "llg_build_h_eff": (C.c_int, [vp, P(_Params), i32, dp]),
+            "llg_compute_demag_field": (C.c_int, [vp, dp]),
+            "llg_step_rk45": (C.c_int, [vp, P(_Params), i32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                        dp, P(i32), dp]),
+            "llg_step_rk23_relax": (C.c_int, [vp, P(_Params), i32, C.c_double, C.c_double, C.c_double,
+                                              C.c_double, dp, P(i32), dp]),
+            "llg_run_rk45": (C.c_int, [vp, P(_Params), i32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                       i64, C.c_double, i64, P(i64), P(i64), dp]),
+            "llg_relax": (C.c_int, [vp, P(_Params), i32, P(RelaxSettings), P(RelaxReport)]),
+            "llg_default_relax_settings": (None, [P(RelaxSettings)]),
+            "llg_compute_energy": (C.c_int, [vp, dp, P(EnergyBreakdown)]),
+            "llg_torque_metric": (C.c_int, [vp, P(_Params), i32, i32, dp]),
+            "llg_demag_kernel_kspace": (C.c_int, [vp, dp]),
+            "llg_init_random": (None, [i64, C.c_uint64, dp]),
+            "llg_init_uniform_with_noise": (None, [i64, dp, C.c_double, C.c_uint64, dp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def declared_symbols(header=None):
+    """Function names declared by the C ABI header include/llg_b200.h."""
+    import re
+    header = header or os.path.join(_HERE, "..", "include", "llg_b200.h")
+    src = re.sub(r"/\*.*?\*/", "", open(header).read(), flags=re.S)
+    return sorted(set(re.findall(r"\b(llg_[a-z0-9_]+)\s*\(", src)))
+
+
+def last_error():
+    buf = C.create_string_buffer(1024)
+    lib().llg_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def _check(rc):
+    if rc != 0:
+        raise LLGError(rc, last_error())
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Grid2D:
+    """Grid2D (grid.rs:4-31)."""
+
+    def __init__(self, nx, ny, dx, dy, dz):
+        self.nx, self.ny, self.dx, self.dy, self.dz = int(nx), int(ny), float(dx), float(dy), float(dz)
+
+    def n_cells(self):
+        return self.nx * self.ny
+
+    def cell_volume(self):
+        return self.dx * self.dy * self.dz
+
+    def _c(self):
+        return _Grid(self.nx, self.ny, self.dx, self.dy, self.dz)
+
+
+class Material:
+    """Material (params.rs:170-184); dmi=None means DMI off."""
+
+    def __init__(self, ms, a_ex, k_u=0.0, easy_axis=(0.0, 0.0, 1.0), dmi=None, demag=False):
+        self.ms, self.a_ex, self.k_u = float(ms), float(a_ex), float(k_u)
+        self.easy_axis = tuple(float(x) for x in easy_axis)
+        self.dmi = None if dmi is None else float(dmi)
+        self.demag = bool(demag)
+
+    def _c(self):
+        return _Material(self.ms, self.a_ex, self.k_u, (C.c_double * 3)(*self.easy_axis),
+                         0.0 if self.dmi is None else self.dmi, 0 if self.dmi is None else 1, 1 if self.demag else 0)
+
+
+class LLGParams:
+    """LLGParams (params.rs:213-219); dt is mutated by the steppers as in the reference."""
+
+    def __init__(self, gamma, alpha, dt, b_ext=(0.0, 0.0, 0.0)):
+        self.gamma, self.alpha, self.dt = float(gamma), float(alpha), float(dt)
+        self.b_ext = tuple(float(x) for x in b_ext)
+
+    def _c(self):
+        return _Params(self.gamma, self.alpha, self.dt, (C.c_double * 3)(*self.b_ext))
+
+
+_ctx_cache = {}
+
+
+def _ctx(device):
+    if device not in _ctx_cache:
+        h = C.c_void_p()
+        _check(lib().llg_ctx_create(int(device), C.byref(h)))
+        _ctx_cache[device] = h
+    return _ctx_cache[device]
+
+
+class Solver:
+    """One film on one GPU: grid + material (+ optional geometry mask), resident m."""
+
+    def __init__(self, grid, material, precision=FP32, geom_mask=None, device=0):
+        self.grid, self.material, self.precision = grid, material, precision
+        self.n = grid.n_cells()
+        mp = None
+        if geom_mask is not None:
+            self._mask = np.ascontiguousarray(np.asarray(geom_mask).reshape(self.n).astype(np.uint8))
+            mp = self._mask.ctypes.data_as(C.c_void_p)
+        h = C.c_void_p()
+        g, m = grid._c(), material._c()
+        _check(lib().llg_solver_create(_ctx(device), C.byref(g), C.byref(m), int(precision), mp, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().llg_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        _check(lib().llg_solver_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def sync(self):
+        _check(lib().llg_solver_sync(self.h))
+
+    def set_state(self, m):
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        assert m.size == 3 * self.n
+        _check(lib().llg_set_state(self.h, _dp(m)))
+
+    def set_state_ptr(self, host_ptr):
+        """Upload from a raw host pointer (e.g. pinned memory) of 3n doubles."""
+        _check(lib().llg_set_state(self.h, C.cast(C.c_void_p(host_ptr), C.POINTER(C.c_double))))
+
+    def get_state(self):
+        out = np.empty((self.n, 3))
+        _check(lib().llg_get_state(self.h, _dp(out)))
+        return out
+
+    def get_state_ptr(self, host_ptr):
+        _check(lib().llg_get_state(self.h, C.cast(C.c_void_p(host_ptr), C.POINTER(C.c_double))))
+
+    def mean_m(self):
+        out = np.empty(3)
+        _check(lib().llg_mean_m(self.h, _dp(out)))
+        return out
+
+    def build_h_eff(self, params, field_mask=FULL):
+        out = np.empty((self.n, 3))
+        p = params._c()
+        _check(lib().llg_build_h_eff(self.h, C.byref(p), int(field_mask), _dp(out)))
+        return out
+
+    def compute_demag_field(self):
+        out = np.empty((self.n, 3))
+        _check(lib().llg_compute_demag_field(self.h, _dp(out)))
+        return out
+
+    def _step(self, fn, params, field_mask, max_err, headroom, dt_min, dt_max):
+        p = params._c()
+        eps, acc, dtu = C.c_double(), C.c_int32(), C.c_double()
+        _check(fn(self.h, C.byref(p), int(field_mask), float(max_err), float(headroom), float(dt_min),
+                  float(dt_max), C.byref(eps), C.byref(acc), C.byref(dtu)))
+        params.dt = p.dt
+        return eps.value, bool(acc.value), dtu.value
+
+    def step_rk45(self, params, field_mask, max_err, headroom, dt_min, dt_max):
+        """step_llg_rk45_recompute_field_masked_adaptive (llg.rs:795): (eps, accepted, dt_used)."""
+        return self._step(lib().llg_step_rk45, params, field_mask, max_err, headroom, dt_min, dt_max)
+
+    def step_rk23_relax(self, params, field_mask, max_err, headroom, dt_min, dt_max):
+        """step_llg_rk23_recompute_field_masked_relax_adaptive (llg.rs:278)."""
+        return self._step(lib().llg_step_rk23_relax, params, field_mask, max_err, headroom, dt_min, dt_max)
+
+    def run_rk45(self, params, field_mask, max_err, headroom, dt_min, dt_max, n_accepted=-1,
+                 t_end=float("inf"), max_attempts=-1):
+        p = params._c()
+        a, r, t = C.c_int64(), C.c_int64(), C.c_double()
+        _check(lib().llg_run_rk45(self.h, C.byref(p), int(field_mask), float(max_err), float(headroom),
+                                  float(dt_min), float(dt_max), int(n_accepted), float(t_end), int(max_attempts),
+                                  C.byref(a), C.byref(r), C.byref(t)))
+        params.dt = p.dt
+        return a.value, r.value, t.value
+
+    def relax(self, params, field_mask, settings):
+        """relax_with_report (relax.rs:334); settings.max_err is written back."""
+        p = params._c()
+        rep = RelaxReport()
+        _check(lib().llg_relax(self.h, C.byref(p), int(field_mask), C.byref(settings), C.byref(rep)))
+        params.dt = p.dt
+        return rep
+
+    def compute_energy(self, b_ext):
+        be = np.ascontiguousarray(np.asarray(b_ext, dtype=np.float64).reshape(3))
+        e = EnergyBreakdown()
+        _check(lib().llg_compute_energy(self.h, _dp(be), C.byref(e)))
+        return e
+
+    def torque_metric(self, params, field_mask, metric=TORQUE_MAX):
+        p = params._c()
+        out = C.c_double()
+        _check(lib().llg_torque_metric(self.h, C.byref(p), int(field_mask), int(metric), C.byref(out)))
+        return out.value
+
+    def kernel_kspace(self):
+        """Real Fourier planes (xx, xy, yy, zz) of K on ky in [0,ny], kx in [0,nx]: shape [4, ny+1, nx+1]."""
+        out = np.empty(4 * (self.grid.nx + 1) * (self.grid.ny + 1))
+        _check(lib().llg_demag_kernel_kspace(self.h, _dp(out)))
+        return out.reshape(4, self.grid.ny + 1, self.grid.nx + 1)
+
+
+def init_random(n, seed):
+    """init_random (initial_states.rs:59-68)."""
+    out = np.empty((int(n), 3))
+    lib().llg_init_random(int(n), C.c_uint64(seed), _dp(out))
+    return out
+
+
+def init_uniform_with_noise(n, direction, noise, seed, m=None):
+    """init_uniform_with_noise (initial_states.rs:43-56); zero cells of `m` are skipped."""
+    out = np.ones((int(n), 3)) if m is None else np.ascontiguousarray(m, dtype=np.float64).copy()
+    d = np.ascontiguousarray(np.asarray(direction, dtype=np.float64).reshape(3))
+    lib().llg_init_uniform_with_noise(int(n), _dp(d), float(noise), C.c_uint64(seed), _dp(out))
+    return out
