@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the uniform-grid LLG hot path on B200: cell-steps/s of FP32 RK45.
+
+Workload (one film per GPU): 1024x1024x1 cells of 2x2x2 nm, Ms 5.8e5 A/m,
+A 1.5e-11 J/m, perpendicular Ku 8e5 J/m^3, interfacial DMI 3e-3 J/m^2,
+alpha 0.3, demag on (open boundaries), seeded random initial m
+(init_random), Dormand-Prince RK45 with max_err 1e-5.  A step is one
+accepted RK45 step of the whole film (six field evaluations, FSAL).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank advances its own film (weak scaling, no data-path
+collective: films are independent); times are the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "llg-sim_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = dict(nx=1024, ny=1024, dx=2e-9, dy=2e-9, dz=2e-9, ms=5.8e5, a_ex=1.5e-11, k_u=8e5,
+                easy=(0.0, 0.0, 1.0), dmi=3e-3, alpha=0.3, seed=1, max_err=1e-5, headroom=0.8, dt0=1e-13,
+                dt_min=1e-18, dt_max=1e-11, b_ext=(0.0, 0.0, 0.0))
+GAMMA = 1.76085963023e11
+# Algorithmic HBM bytes per cell per accepted FP32 RK45 step (six evaluations):
+# per evaluation m_s 12 + k_s 12 + m0 12 + spectral round trips 96 + kernel 16 = 148,
+# plus 12 B per previous torque in the stage combinations, the error-norm reads
+# and the accepted state: 6*148 + 240 + 60 + 12 = 1200.
+BYTES_PER_CELL_STEP = 1200
+METRIC = "cell-steps/s FP32 vs FP64 at 1e-4 <m>; relax wall-time learned vs plain start"
+UNIT = "cell-steps/s"
+
+
+def workload_desc():
+    w = WORKLOAD
+    return (f"{w['nx']}x{w['ny']}x1 film, {w['dx']*1e9:.0f}x{w['dy']*1e9:.0f}x{w['dz']*1e9:.0f} nm cells, "
+            f"Ms {w['ms']:.2e}, A {w['a_ex']:.2e}, Ku {w['k_u']:.0e} (+z), D {w['dmi']:.0e}, alpha {w['alpha']}, "
+            f"demag on, random m0 (seed {w['seed']}), RK45 max_err {w['max_err']:.0e}")
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_env():
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 oracle (C++ restatement of the reference path)
+# ---------------------------------------------------------------------------
+def cpu_baseline(budget_s=20.0, warmup_steps=0):
+    import oracle as O
+
+    w = WORKLOAD
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    n = w["nx"] * w["ny"]
+    g = O.make_grid(w["nx"], w["ny"], w["dx"], w["dy"], w["dz"])
+    mat = O.make_material(w["ms"], w["a_ex"], w["k_u"], w["easy"], w["dmi"], True)
+    s = O.Solver(g, mat)
+    m = O.init_random(n, w["seed"])
+    p = O.make_params(GAMMA, w["alpha"], w["dt0"], w["b_ext"])
+    s.build_h_eff(m, w["b_ext"], 2)  # builds the cached demag operator (untimed, as the reference caches it)
+    args = (2, w["max_err"], w["headroom"], w["dt_min"], w["dt_max"])
+    for _ in range(warmup_steps):
+        s.step_rk45(m, p, *args)
+    acc = rej = 0
+    t0 = time.perf_counter()
+    while True:
+        _, a, _ = s.step_rk45(m, p, *args)
+        acc += a
+        rej += not a
+        el = time.perf_counter() - t0
+        if acc >= 1 and el >= budget_s:
+            break
+    return {"value": n * acc / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{w['nx']}x{w['ny']} film of the same workload, FP64 oracle (C++ restatement, demag "
+                      f"FFT OpenMP-parallel, local terms serial as in the reference), {acc} accepted + {rej} "
+                      f"rejected RK45 steps in {el:.1f} s"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    budget = 90.0
+    import oracle as O
+
+    w = WORKLOAD
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    n = w["nx"] * w["ny"]
+    g = O.make_grid(w["nx"], w["ny"], w["dx"], w["dy"], w["dz"])
+    s = O.Solver(g, O.make_material(w["ms"], w["a_ex"], w["k_u"], w["easy"], w["dmi"], True))
+    m = O.init_random(n, w["seed"])
+    p = O.make_params(GAMMA, w["alpha"], w["dt0"], w["b_ext"])
+    s.build_h_eff(m, w["b_ext"], 2)
+    sargs = (2, w["max_err"], w["headroom"], w["dt_min"], w["dt_max"])
+    for _ in range(min(args.warmup, 1)):
+        s.step_rk45(m, p, *sargs)
+    acc = rej = 0
+    t0 = time.perf_counter()
+    while acc < args.steps:
+        _, a, _ = s.step_rk45(m, p, *sargs)
+        acc += a
+        rej += not a
+        if time.perf_counter() - t0 > budget and acc >= 1:
+            break
+    el = time.perf_counter() - t0
+    value = n * acc / el
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": acc, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * el / acc, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_desc(), "cells": n, "precision": "fp64 (reference arithmetic)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{acc} accepted (+{rej} rejected) RK45 steps of the full film, bounded "
+                                       f"to ~{budget:.0f} s; oracle C++ restatement (the Rust reference cannot "
+                                       f"be compiled here)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def make_solver(L, precision):
+    w = WORKLOAD
+    g = L.Grid2D(w["nx"], w["ny"], w["dx"], w["dy"], w["dz"])
+    mat = L.Material(w["ms"], w["a_ex"], w["k_u"], w["easy"], w["dmi"], True)
+    return L.Solver(g, mat, precision)
+
+
+def params(L):
+    w = WORKLOAD
+    return L.LLGParams(GAMMA, w["alpha"], w["dt0"], w["b_ext"])
+
+
+def run_gpu(args):
+    import torch
+
+    import llg_b200 as L
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = WORKLOAD
+    n = w["nx"] * w["ny"]
+    fm = L.FULL
+    ctl = (w["max_err"], w["headroom"], w["dt_min"], w["dt_max"])
+    m0 = L.init_random(n, w["seed"] + rank)
+    stream = torch.cuda.Stream()
+    s = make_solver(L, L.FP32)
+    s.set_stream(stream.cuda_stream)
+    s.set_state(m0)
+    p = params(L)
+    # warm-up (graph capture, clocks) — untimed
+    s.run_rk45(p, fm, *ctl, n_accepted=args.warmup)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = s.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    acc, rej, t_adv = s.run_rk45(p, fm, *ctl, n_accepted=args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_local = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    launches = s.launch_count() - launches0
+    ms = max_over_ranks(ms_local)
+    value = n * acc * world / (ms * 1e-3)
+    step_ms = ms / acc
+    peak, peak_kind = peaks()
+
+    # per-kernel roofline of one RK45 stage (same state, CUDA events per pass)
+    prof = s.profile_stage(p, fm, reps=30)
+    K1 = w["nx"] + 1
+    x_bytes = 3 * K1 * w["ny"] * 8
+    khat_bytes = K1 * (w["ny"] + 1) * 16
+    plane = 3 * n * 4
+    bytes_pass = {"k_row_forward": plane * (1 + 3 + 1) + x_bytes,   # m0 + 3 torques + m_s out + X out
+                  "k_column": 2 * x_bytes + khat_bytes,            # X in/out + kernel planes
+                  "k_row_inverse": x_bytes + 2 * plane}            # X in + m_s in + k out
+    names = ["k_row_forward", "k_column", "k_row_inverse"]
+    dom = names[int(np.argmax(prof))]
+    dom_ms = float(prof[names.index(dom)])
+    achieved = bytes_pass[dom] / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if os.path.exists(tpath):
+        for line in open(tpath):
+            if line.startswith(dom + " "):
+                try:
+                    traffic = float(line.split()[1])
+                except ValueError:
+                    pass
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "bytes_per_launch": bytes_pass[dom], "ms_per_launch": dom_ms,
+                "per_pass_ms": {k: float(v) for k, v in zip(names, prof)},
+                "per_pass_frac": {k: bytes_pass[k] / (float(v) * 1e-3) / 1e9 / peak for k, v in zip(names, prof)}}
+    step_ach = BYTES_PER_CELL_STEP * n * acc / (ms_local * 1e-3) / 1e9
+    roofline_step = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s", "frac": step_ach / peak,
+                     "bytes_per_cell_step": BYTES_PER_CELL_STEP, "peak_source": peak_kind}
+
+    # end to end through the reference-facing call with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_m = torch.from_numpy(m0.copy()).pin_memory()
+        host_out = torch.empty_like(host_m).pin_memory()
+        s2 = make_solver(L, L.FP32)
+        s2.set_stream(stream.cuda_stream)
+        p2 = params(L)
+        s2.set_state_ptr(host_m.data_ptr())
+        s2.run_rk45(p2, fm, *ctl, n_accepted=args.warmup)  # warm the graphs
+        p2 = params(L)
+        k_e2e = max(1, min(args.steps, 100))
+        torch.cuda.synchronize()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        f0.record(stream)
+        s2.set_state_ptr(host_m.data_ptr())
+        acc2 = 0
+        calls = 0
+        while acc2 < k_e2e:
+            _, a, _ = s2.step_rk45(p2, fm, *ctl)
+            acc2 += a
+            calls += 1
+        s2.get_state_ptr(host_out.data_ptr())
+        f1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        ms_e2e = max_over_ranks(max(f0.elapsed_time(f1), wall * 1e3))
+        state_bytes = n * 3 * 8
+        e2e = {"value": n * acc2 * world / (ms_e2e * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes / acc2, "d2h_bytes_per_step": (state_bytes + 192 * calls) / acc2,
+               "steps": acc2, "calls": calls,
+               "path": "llg_set_state (pinned AoS f64) + llg_step_rk45 per attempt (host params in, eps/accepted/"
+                       "dt out) + llg_get_state"}
+        s2.close()
+
+    # FP32 vs FP64 at matched simulated time from the same initial state
+    fp64 = None
+    if not args.no_fp64:
+        k64 = max(1, min(args.steps, 60))
+        a32 = make_solver(L, L.FP32)
+        a64 = make_solver(L, L.FP64)
+        for sv in (a32, a64):
+            sv.set_stream(stream.cuda_stream)
+            sv.set_state(m0)
+        pa = params(L)
+        acc32, _, t32 = a32.run_rk45(pa, fm, *ctl, n_accepted=k64)
+        pb = params(L)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        acc64, rej64, t64 = a64.run_rk45(pb, fm, *ctl, t_end=t32)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = g0.elapsed_time(g1)
+        # FP32 to the same time (its own dt sequence), compare <m>
+        a32.set_state(m0)
+        pa = params(L)
+        a32.run_rk45(pa, fm, *ctl, t_end=t32)
+        d = np.abs(a32.mean_m() - a64.mean_m()).max()
+        fp64 = {"value": n * acc64 * world / (ms64 * 1e-3), "unit": UNIT, "accepted": acc64, "rejected": rej64,
+                "t_sim": t64, "mean_m_max_abs_diff_vs_fp32": float(d), "tolerance": 1e-4}
+        a32.close()
+        a64.close()
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_budget)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": acc, "warmup": args.warmup,
+                "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": workload_desc(), "cells_per_gpu": n, "global_cells": n * world,
+                           "parallelism": f"independent films, 1 per GPU x{world}", "rejected_steps": rej,
+                           "t_sim_s": t_adv,
+                           "l2": "inputs larger than L2: ~190 MB per film working set (m, 7 torques, stage states, "
+                                 "25 MB spectrum, 16 MB kernel) vs 126 MB L2"},
+                "clocks": clk, "gpu_launches": launches, "roofline": roofline, "roofline_step": roofline_step,
+                "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

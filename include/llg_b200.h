@@ -155,7 +155,7 @@ int llg_step_rk23_relax(llg_solver* s, llg_params* params, int32_t field_mask, d
 
 /* Device-resident RK45 integration: repeats attempts on the GPU without host
  * round trips until `n_accepted` more steps are accepted or the simulated time
- * reaches t_end (dt is clamped to land on t_end, as the drivers do in
+ * reaches t_end, measured from the start of this call (dt is clamped to land on t_end, as the drivers do in
  * st_problems/sp4.rs:308-314).  Pass n_accepted < 0 or t_end = +inf to disable
  * either limit.  max_attempts bounds the work. */
 int llg_run_rk45(llg_solver* s, llg_params* params, int32_t field_mask, double max_err, double headroom,
@@ -177,6 +177,14 @@ int llg_torque_metric(llg_solver* s, const llg_params* params, int32_t field_mas
  * K = mu0 * N on kx in [0,nx], ky in [0,ny], as FP64, without the 1/(px*py)
  * scaling (compare with the real part of Demag2D::kxx.. at those indices). */
 int llg_demag_kernel_kspace(llg_solver* s, double* out /* 4*(nx+1)*(ny+1) */);
+
+/* ---------------- instrumentation (no reference counterpart) ----------------
+ * llg_profile_stage: CUDA-event timing of the three passes of one RK45 stage
+ * evaluation (row forward, column, row inverse), averaged over `reps`
+ * launches on the solver stream; ms3 receives milliseconds per pass.
+ * llg_solver_launch_count: kernels this solver has issued so far. */
+int llg_profile_stage(llg_solver* s, const llg_params* params, int32_t field_mask, int32_t reps, double* ms3);
+int llg_solver_launch_count(llg_solver* s, int64_t* out);
 
 /* ---------------- initial states (initial_states.rs) ---------------- */
 void llg_init_random(int64_t n, uint64_t seed, double* m_aos);                   /* :59-68 */

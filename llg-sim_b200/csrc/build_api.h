@@ -36,5 +36,8 @@ template <typename R>
 cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s);
 template <typename R>
 cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col);
+// Launches one pass of an evaluation: 0 = row forward, 1 = column, 2 = row inverse.
+template <typename R>
+cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s);
 
 }  // namespace llg

@@ -30,6 +30,16 @@ cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t 
     return cudaGetLastError();
 }
 
+template <typename R>
+cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s) {
+    if (which == 0) k_row_forward<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+    else if (which == 1) k_column<R><<<g.grid_col, 256, g.smem_col, s>>>(g.films, g.col_items, g.n_col_items, spec);
+    else k_row_inverse<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_one<float>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t);
+template cudaError_t launch_one<double>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t);
 template cudaError_t prepare_eval_kernels<float>(size_t, size_t);
 template cudaError_t prepare_eval_kernels<double>(size_t, size_t);
 template cudaError_t launch_eval<float>(const EvalSpec&, const LaunchGeom&, cudaStream_t);

@@ -222,6 +222,8 @@ struct EngineBase {
     virtual int energy(const double* bext, llg_energy_breakdown* out) = 0;
     virtual int torque_metric(const llg_params* p, int fmask, int metric, double* out) = 0;
     virtual int kernel_kspace(double* out) = 0;
+    virtual int profile_stage(const llg_params* p, int fmask, int reps, double* ms3) = 0;
+    virtual long long launch_count() = 0;
 };
 
 template <typename R>
@@ -251,6 +253,14 @@ struct Engine final : EngineBase {
     bool last_b_eff_valid = false;  // relax: torque stats of the resident state are current
     std::map<long long, cudaGraphExec_t> graphs;
     std::map<long long, cudaGraph_t> graph_defs;
+    std::map<long long, long long> graph_kernels;  // kernel nodes per graph
+    long long launches = 0;                         // kernels issued on the stream so far
+
+    int eval(const EvalSpec& e) {
+        CUDA_TRY(launch_eval<R>(e, geom, stream));
+        launches += (e.demag && geom.any_demag) ? 3 : 2;
+        return LLG_OK;
+    }
 
     ~Engine() override {
         if (stream) cudaStreamSynchronize(stream);
@@ -411,6 +421,7 @@ struct Engine final : EngineBase {
         c.invalidate_fsal = 1;
         k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
         CUDA_TRY(cudaGetLastError());
+        launches += 1;
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
     }
@@ -505,25 +516,25 @@ struct Engine final : EngineBase {
         e.rhs = rhs;
         e.k_out = KB_K1;
         e.skip_if_fsal = 1;
-        CUDA_TRY(launch_eval<R>(e, geom, stream));
+        { int _rc = eval(e); if (_rc) return _rc; }
         e.skip_if_fsal = 0;
         if (kind == KIND_RK45) {
             using namespace dp5;
             combo(e, MB_S0, {KB_K1}, {A21});
             e.k_out = KB_K2;
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             combo(e, MB_S1, {KB_K1, KB_K2}, {A31, A32});
             e.k_out = KB_K3;
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             combo(e, MB_S0, {KB_K1, KB_K2, KB_K3}, {A41, A42, A43});
             e.k_out = KB_K4;
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             combo(e, MB_S1, {KB_K1, KB_K2, KB_K3, KB_K4}, {A51, A52, A53, A54});
             e.k_out = KB_K5;
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             combo(e, MB_S0, {KB_K1, KB_K2, KB_K3, KB_K4, KB_K5}, {A61, A62, A63, A64, A65});
             e.k_out = KB_K6;
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             combo(e, MB_M7, {KB_K1, KB_K3, KB_K4, KB_K5, KB_K6}, {B1, B3, B4, B5, B6});
             e.k_out = KB_K7;
             e.err = ERR_RK45;
@@ -531,17 +542,18 @@ struct Engine final : EngineBase {
             const double wh[8] = {0, BH1, 0, BH3, BH4, BH5, BH6, BH7};
             std::memcpy(e.wb, wb, sizeof(wb));
             std::memcpy(e.wh, wh, sizeof(wh));
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             k_controller<<<1, 32, 0, stream>>>(d_film, 1, 5);
             CUDA_TRY(cudaGetLastError());
+            launches += 1;
         } else {
             using namespace bs3;
             combo(e, MB_S0, {KB_K1}, {A21});
             e.k_out = KB_K2;
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             combo(e, MB_S1, {KB_K2}, {A32});
             e.k_out = KB_K3;
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             combo(e, MB_M7, {KB_K1, KB_K2, KB_K3}, {B1, B2, B3});
             e.k_out = KB_K7;
             e.err = ERR_RK23;
@@ -550,18 +562,29 @@ struct Engine final : EngineBase {
             const double wh[8] = {0, BH1, BH2, BH3, BH4, 0, 0, 0};
             std::memcpy(e.wb, wb, sizeof(wb));
             std::memcpy(e.wh, wh, sizeof(wh));
-            CUDA_TRY(launch_eval<R>(e, geom, stream));
+            { int _rc = eval(e); if (_rc) return _rc; }
             k_controller<<<1, 32, 0, stream>>>(d_film, 1, 3);
             CUDA_TRY(cudaGetLastError());
             k_finalize<<<1, 32, 0, stream>>>(d_film, 1);
             CUDA_TRY(cudaGetLastError());
+            launches += 2;
         }
         return LLG_OK;
     }
 
+    int graph_launch(long long key, cudaGraphExec_t ge) {
+        CUDA_TRY(cudaGraphLaunch(ge, stream));
+        launches += graph_kernels[key];
+        return LLG_OK;
+    }
+
     // Graph of `reps` back-to-back attempts.
+    static long long graph_key(int kind, int fmask, int reps) {
+        return ((long long)kind << 40) | ((long long)fmask << 32) | (long long)reps;
+    }
+
     int attempt_graph(int kind, int fmask, int reps, cudaGraphExec_t* out) {
-        long long key = ((long long)kind << 40) | ((long long)fmask << 32) | (long long)reps;
+        long long key = graph_key(kind, fmask, reps);
         auto it = graphs.find(key);
         if (it != graphs.end()) {
             *out = it->second;
@@ -573,7 +596,10 @@ struct Engine final : EngineBase {
         cudaStream_t saved = stream;
         stream = cap;
         int rc = LLG_OK;
+        const long long before = launches;
         for (int r = 0; r < reps && rc == LLG_OK; ++r) rc = launch_attempt(kind, fmask);
+        graph_kernels[key] = launches - before;
+        launches = before;
         stream = saved;
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(cap, &g);
@@ -620,9 +646,10 @@ struct Engine final : EngineBase {
         if (rc) return rc;
         k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
         CUDA_TRY(cudaGetLastError());
+        launches += 1;
         cudaGraphExec_t ge = nullptr;
         if ((rc = attempt_graph(kind, fmask, 1, &ge))) return rc;
-        CUDA_TRY(cudaGraphLaunch(ge, stream));
+        if ((rc = graph_launch(graph_key(kind, fmask, 1), ge))) return rc;
         if ((rc = read_state())) return rc;
         const StepState& s = *h_state;
         if (s.err_code) {
@@ -659,6 +686,7 @@ struct Engine final : EngineBase {
         if ((rc = prepare_step(kind, p, fmask, &c))) return rc;
         k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
         CUDA_TRY(cudaGetLastError());
+        launches += 1;
         const int reps = 8;
         cudaGraphExec_t ge = nullptr;
         if ((rc = attempt_graph(kind, fmask, reps, &ge))) return rc;
@@ -667,7 +695,7 @@ struct Engine final : EngineBase {
         for (;;) {
             // several graph launches between polls
             for (int q = 0; q < 4 && launched < limit; ++q) {
-                CUDA_TRY(cudaGraphLaunch(ge, stream));
+                if ((rc = graph_launch(graph_key(kind, fmask, reps), ge))) return rc;
                 launched += reps;
             }
             if ((rc = read_state())) return rc;
@@ -707,7 +735,8 @@ struct Engine final : EngineBase {
         c.dt = h_state->dt;
         k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(launch_eval<R>(e, geom, stream));
+        launches += 1;
+        { int _rc = eval(e); if (_rc) return _rc; }
         if (e.reduce) {
             k_finalize<<<1, 32, 0, stream>>>(d_film, 1);
             CUDA_TRY(cudaGetLastError());
@@ -793,6 +822,48 @@ struct Engine final : EngineBase {
         *out = metric_from(*h_state, metric);
         return LLG_OK;
     }
+
+    // Per-kernel CUDA-event timing of one representative RK45 stage evaluation
+    // (stage 4: three-term combination) repeated `reps` times on the stream.
+    int profile_stage(const llg_params* p, int fmask, int reps, double* ms3) override {
+        int rc;
+        if ((rc = apply_params(p, nullptr))) return rc;
+        Control c = idle_control();
+        if ((rc = read_state())) return rc;
+        c.dt = h_state->dt > 0 ? h_state->dt : p->dt;
+        k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
+        CUDA_TRY(cudaGetLastError());
+        EvalSpec e = base_spec(fmask);
+        e.rhs = RHS_LLG;
+        combo(e, MB_S0, {KB_K1, KB_K2, KB_K3}, {dp5::A41, dp5::A42, dp5::A43});
+        e.k_out = KB_K4;
+        cudaEvent_t ev[4];
+        for (auto& x : ev) CUDA_TRY(cudaEventCreate(&x));
+        double acc[3] = {0, 0, 0};
+        for (int r = 0; r < reps; ++r) {
+            CUDA_TRY(cudaEventRecord(ev[0], stream));
+            k_row_forward_launch(e);
+            CUDA_TRY(cudaEventRecord(ev[1], stream));
+            if (e.demag && geom.any_demag) k_column_launch(e);
+            CUDA_TRY(cudaEventRecord(ev[2], stream));
+            k_row_inverse_launch(e);
+            CUDA_TRY(cudaEventRecord(ev[3], stream));
+            CUDA_TRY(cudaEventSynchronize(ev[3]));
+            for (int q = 0; q < 3; ++q) {
+                float ms = 0.f;
+                CUDA_TRY(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+                acc[q] += ms;
+            }
+        }
+        for (auto& x : ev) cudaEventDestroy(x);
+        for (int q = 0; q < 3; ++q) ms3[q] = acc[q] / reps;
+        return LLG_OK;
+    }
+    void k_row_forward_launch(const EvalSpec& e) { launch_one<R>(0, e, geom, stream); }
+    void k_column_launch(const EvalSpec& e) { launch_one<R>(1, e, geom, stream); }
+    void k_row_inverse_launch(const EvalSpec& e) { launch_one<R>(2, e, geom, stream); }
+
+    long long launch_count() override { return launches; }
 
     int kernel_kspace(double* out) override {
         if (!mat.demag || !d_k64) return set_error(LLG_ERR_INVALID, "material has demag disabled");
@@ -1175,6 +1246,19 @@ int llg_demag_kernel_kspace(llg_solver* s, double* out) {
     int rc = bind(s);
     if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");
     return rc ? rc : s->eng->kernel_kspace(out);
+}
+
+int llg_profile_stage(llg_solver* s, const llg_params* p, int32_t fmask, int32_t reps, double* ms3) {
+    int rc = bind(s);
+    if (!rc && (!p || !ms3 || reps < 1)) rc = set_error(LLG_ERR_INVALID, "bad argument");
+    return rc ? rc : s->eng->profile_stage(p, fmask, reps, ms3);
+}
+int llg_solver_launch_count(llg_solver* s, int64_t* out) {
+    int rc = bind(s);
+    if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");
+    if (rc) return rc;
+    *out = s->eng->launch_count();
+    return LLG_OK;
 }
 
 // XorShift64 seeded initial states (initial_states.rs:43-68, 230-254).

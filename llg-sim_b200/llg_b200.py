@@ -133,6 +133,8 @@ def lib():
             "llg_compute_energy": (C.c_int, [vp, dp, P(EnergyBreakdown)]),
             "llg_torque_metric": (C.c_int, [vp, P(_Params), i32, i32, dp]),
             "llg_demag_kernel_kspace": (C.c_int, [vp, dp]),
+            "llg_profile_stage": (C.c_int, [vp, P(_Params), i32, i32, dp]),
+            "llg_solver_launch_count": (C.c_int, [vp, P(i64)]),
             "llg_init_random": (None, [i64, C.c_uint64, dp]),
             "llg_init_uniform_with_noise": (None, [i64, dp, C.c_double, C.c_uint64, dp]),
         }
@@ -328,6 +330,18 @@ class Solver:
         p = params._c()
         out = C.c_double()
         _check(lib().llg_torque_metric(self.h, C.byref(p), int(field_mask), int(metric), C.byref(out)))
+        return out.value
+
+    def profile_stage(self, params, field_mask=FULL, reps=20):
+        """Milliseconds per pass (row forward, column, row inverse) of one RK45 stage."""
+        p = params._c()
+        out = np.empty(3)
+        _check(lib().llg_profile_stage(self.h, C.byref(p), int(field_mask), int(reps), _dp(out)))
+        return out
+
+    def launch_count(self):
+        out = C.c_int64()
+        _check(lib().llg_solver_launch_count(self.h, C.byref(out)))
         return out.value
 
     def kernel_kspace(self):

@@ -1,0 +1,42 @@
+"""CPU checks of the C ABI library: it loads, exports every symbol the header
+declares, reports errors through statuses, and its host-side input generators
+match the oracle bit for bit.  No GPU compute is called here."""
+import ctypes as C
+
+import numpy as np
+
+
+def test_library_exports_every_declared_symbol(gpu):
+    names = gpu.declared_symbols()
+    assert len(names) >= 20
+    lib = C.CDLL(gpu.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version(gpu):
+    assert gpu.lib().llg_abi_version() == 1
+
+
+def test_errors_are_statuses_not_aborts(gpu):
+    import torch
+
+    h = C.c_void_p()
+    rc = gpu.lib().llg_ctx_create(-1 if torch.cuda.is_available() else 0, C.byref(h))
+    assert rc in (-1, -6)  # LLG_ERR_INVALID / LLG_ERR_NO_DEVICE
+    assert len(gpu.last_error()) > 0
+
+
+def test_init_generators_match_oracle(gpu, orc):
+    assert np.array_equal(gpu.init_random(500, 77), orc.init_random(500, 77))
+    base = np.ones((64, 3))
+    base[::7] = 0.0
+    assert np.array_equal(gpu.init_uniform_with_noise(64, (0, 1, 1), 0.1, 5, base),
+                          orc.init_uniform_with_noise(64, (0, 1, 1), 0.1, 5, base))
+
+
+def test_default_relax_settings_match_oracle(gpu, orc):
+    a = gpu.RelaxSettings.default()
+    b = orc.default_relax_settings()
+    for name, _ in gpu.RelaxSettings._fields_:
+        assert getattr(a, name) == getattr(b, name), name
