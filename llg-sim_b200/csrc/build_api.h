@@ -30,7 +30,24 @@ struct LaunchGeom {
     int grid_row;
     int grid_col;
     bool any_demag;
+    int fast_row;     // register-FFT row kernels for L = nx (0: generic kernels)
+    int fast_col;     // register-FFT column kernel for L = ny (0: generic kernel)
+    int row_threads;
+    int col_threads;
 };
+
+// Register-FFT configuration for a film size: rows per block T, columns per
+// block, threads and shared memory; ok = false when the size has no fast path.
+struct FastCfg {
+    bool ok;
+    int T, NC, row_threads, col_threads;
+    size_t smem_row, smem_col;
+    int twp_row_size, twp_col_size;
+};
+template <typename R>
+FastCfg fast_config(int nx, int ny);
+template <typename R>
+cudaError_t build_pass_tables(void* out_row, int nx, void* out_col, int ny, cudaStream_t s);
 
 template <typename R>
 cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s);

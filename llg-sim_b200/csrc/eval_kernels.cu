@@ -1,9 +1,73 @@
 // eval_kernels.cu — instantiation and launch of the per-evaluation kernels for
-// FP32 and FP64.
+// FP32 and FP64: register-FFT kernels for power-of-two sizes, generic
+// shared-memory Stockham kernels otherwise.
 #include "build_api.h"
-#include "field_kernels.cuh"
+#include "fast_kernels.cuh"
 
 namespace llg {
+
+namespace {
+
+template <typename R, typename F>
+bool dispatch_L(int L, F&& f) {
+    switch (L) {
+        case 16: f(std::integral_constant<int, 16>{}); return true;
+        case 32: f(std::integral_constant<int, 32>{}); return true;
+        case 64: f(std::integral_constant<int, 64>{}); return true;
+        case 128: f(std::integral_constant<int, 128>{}); return true;
+        case 256: f(std::integral_constant<int, 256>{}); return true;
+        case 512: f(std::integral_constant<int, 512>{}); return true;
+        case 1024: f(std::integral_constant<int, 1024>{}); return true;
+        case 2048: f(std::integral_constant<int, 2048>{}); return true;
+        default: return false;
+    }
+}
+
+constexpr size_t kSmemMax = 227 * 1024;
+
+}  // namespace
+
+template <typename R>
+FastCfg fast_config(int nx, int ny) {
+    FastCfg c{};
+    bool okr = dispatch_L<R>(nx, [&](auto LC) {
+        constexpr int L = decltype(LC)::value;
+        c.T = RowCfg<R, L>::T;
+        c.row_threads = RowCfg<R, L>::THREADS;
+        c.smem_row = RowCfg<R, L>::SMEM;
+        c.twp_row_size = TwTab<R, L>::size;
+    });
+    bool okc = dispatch_L<R>(ny, [&](auto LC) {
+        constexpr int L = decltype(LC)::value;
+        c.NC = ColCfg<R, L>::NC;
+        c.col_threads = ColCfg<R, L>::THREADS;
+        c.smem_col = ColCfg<R, L>::SMEM;
+        c.twp_col_size = TwTab<R, L>::size;
+    });
+    c.ok = okr && okc && c.smem_row <= kSmemMax && c.smem_col <= kSmemMax;
+    return c;
+}
+
+template <typename R>
+cudaError_t build_pass_tables(void* out_row, int nx, void* out_col, int ny, cudaStream_t s) {
+    cudaError_t err = cudaSuccess;
+    dispatch_L<R>(nx, [&](auto LC) {
+        constexpr int L = decltype(LC)::value;
+        if (TwTab<R, L>::size > 0) {
+            k_pass_tables<R, L><<<(TwTab<R, L>::size + 255) / 256, 256, 0, s>>>(reinterpret_cast<cx<R>*>(out_row));
+            err = cudaGetLastError();
+        }
+    });
+    if (err != cudaSuccess) return err;
+    dispatch_L<R>(ny, [&](auto LC) {
+        constexpr int L = decltype(LC)::value;
+        if (TwTab<R, L>::size > 0) {
+            k_pass_tables<R, L><<<(TwTab<R, L>::size + 255) / 256, 256, 0, s>>>(reinterpret_cast<cx<R>*>(out_col));
+            err = cudaGetLastError();
+        }
+    });
+    return err;
+}
 
 template <typename R>
 cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
@@ -13,31 +77,74 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
     e = cudaFuncSetAttribute(k_row_inverse<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_col);
-    return e;
-}
-
-template <typename R>
-cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s) {
-    k_row_forward<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
-    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (spec.demag && g.any_demag) {
-        k_column<R><<<g.grid_col, 256, g.smem_col, s>>>(g.films, g.col_items, g.n_col_items, spec);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
-    k_row_inverse<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+    // fast kernels: every instantiation whose shared memory fits
+    auto set_all = [&](auto LC) {
+        constexpr int L = decltype(LC)::value;
+        if (RowCfg<R, L>::SMEM <= kSmemMax) {
+            cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)RowCfg<R, L>::SMEM);
+            cudaFuncSetAttribute(k_row_inverse_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)RowCfg<R, L>::SMEM);
+        }
+        if (ColCfg<R, L>::SMEM <= kSmemMax)
+            cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ColCfg<R, L>::SMEM);
+    };
+    for (int L : {16, 32, 64, 128, 256, 512, 1024, 2048}) dispatch_L<R>(L, set_all);
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s) {
-    if (which == 0) k_row_forward<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
-    else if (which == 1) k_column<R><<<g.grid_col, 256, g.smem_col, s>>>(g.films, g.col_items, g.n_col_items, spec);
-    else k_row_inverse<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+    if (which == 0 || which == 2) {
+        if (g.fast_row) {
+            dispatch_L<R>(g.fast_row, [&](auto LC) {
+                constexpr int L = decltype(LC)::value;
+                if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
+                    if (which == 0)
+                        k_row_forward_fast<R, L><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                            g.films, g.row_items, g.n_row_items, spec);
+                    else
+                        k_row_inverse_fast<R, L><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                            g.films, g.row_items, g.n_row_items, spec);
+                }
+            });
+        } else if (which == 0) {
+            k_row_forward<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+        } else {
+            k_row_inverse<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+        }
+    } else {
+        if (g.fast_col) {
+            dispatch_L<R>(g.fast_col, [&](auto LC) {
+                constexpr int L = decltype(LC)::value;
+                if constexpr (ColCfg<R, L>::SMEM <= kSmemMax)
+                    k_column_fast<R, L><<<g.grid_col, ColCfg<R, L>::THREADS, ColCfg<R, L>::SMEM, s>>>(
+                        g.films, g.col_items, g.n_col_items, spec);
+            });
+        } else {
+            k_column<R><<<g.grid_col, 256, g.smem_col, s>>>(g.films, g.col_items, g.n_col_items, spec);
+        }
+    }
     return cudaGetLastError();
 }
 
+template <typename R>
+cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s) {
+    cudaError_t e = launch_one<R>(0, spec, g, s);
+    if (e != cudaSuccess) return e;
+    if (spec.demag && g.any_demag) {
+        e = launch_one<R>(1, spec, g, s);
+        if (e != cudaSuccess) return e;
+    }
+    return launch_one<R>(2, spec, g, s);
+}
+
+template FastCfg fast_config<float>(int, int);
+template FastCfg fast_config<double>(int, int);
+template cudaError_t build_pass_tables<float>(void*, int, void*, int, cudaStream_t);
+template cudaError_t build_pass_tables<double>(void*, int, void*, int, cudaStream_t);
 template cudaError_t launch_one<float>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t);
 template cudaError_t launch_one<double>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t);
 template cudaError_t prepare_eval_kernels<float>(size_t, size_t);

@@ -410,70 +410,15 @@ __global__ void __launch_bounds__(256) k_column(const FilmDev* __restrict__ film
     }
 }
 
-// ---------------------------------------------------------------------------
-// Pass 3: C2R along x + local terms + torque + error norm + reductions.
-// ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(256) k_row_inverse(const FilmDev* __restrict__ films,
-                                                     const WorkItem* __restrict__ items, int nitems, EvalSpec spec) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double sm_red[32 * RED_NSLOT];
-    cx<R>* sm = reinterpret_cast<cx<R>*>(smem_raw);
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const WorkItem w = items[it];
-        const FilmDev& F = films[w.film];
-        StepState* st = F.st;
-        if (!st->active) continue;
-        if (spec.skip_if_fsal && st->fsal_valid) continue;
-        const int nx = F.nx, ny = F.ny, n = nx * ny, T = F.rows_per_block;
-        const int j0 = w.blk * T;
-        const int cur = st->cur;
-        const int L = nx, K1 = nx + 1, L2 = 2 * nx;
-        const int G = T + (T + 1) / 2, P = (T + 1) / 2;
-        const bool do_fft = spec.demag && F.demag_mat;
-        const cx<R>* __restrict__ tw = reinterpret_cast<const cx<R>*>(F.tw_row);
-        R* D = nullptr;
-        if (do_fft) {
-            const cx<R>* __restrict__ X = reinterpret_cast<const cx<R>*>(F.X);
-            cx<R>* A = sm;
-            cx<R>* B = sm + 2 * G * L;
-            auto xval = [&](int c, int k, int j) -> cx<R> {
-                if (k <= nx) return X[(c * K1 + k) * ny + j];
-                return conjc(X[(c * K1 + (L2 - k)) * ny + j]);
-            };
-            for (int e = threadIdx.x; e < L2 * T; e += blockDim.x) {
-                const int r = e % T, k = e / T, j = j0 + r;
-                cx<R> z = mkc((R)0, (R)0);
-                if (j < ny) {
-                    cx<R> bx = xval(0, k, j), by = xval(1, k, j);
-                    z = mkc(bx.re - by.im, bx.im + by.re);
-                }
-                A[(2 * r + (k & 1)) * L + (k >> 1)] = z;
-            }
-            for (int e = threadIdx.x; e < L2 * P; e += blockDim.x) {
-                const int p = e % P, k = e / P;
-                const int ja = j0 + 2 * p, jb = j0 + 2 * p + 1;
-                cx<R> za = (ja < ny) ? xval(2, k, ja) : mkc((R)0, (R)0);
-                cx<R> zb = (2 * p + 1 < T && jb < ny) ? xval(2, k, jb) : mkc((R)0, (R)0);
-                A[(2 * (T + p) + (k & 1)) * L + (k >> 1)] = mkc(za.re - zb.im, za.im + zb.re);
-            }
-            __syncthreads();
-            cx<R>* res = fft_smem<R>(A, B, 2 * G, F.plan_row, tw, true);
-            D = reinterpret_cast<R*>(res == A ? B : A);
-            for (int e = threadIdx.x; e < G * L; e += blockDim.x) {
-                const int g = e / L, x = e - g * L;
-                cx<R> z = res[(2 * g) * L + x] + cmulc(res[(2 * g + 1) * L + x], tw[x]);
-                if (g < T) {
-                    D[(g * 3 + 0) * L + x] = z.re;
-                    D[(g * 3 + 1) * L + x] = z.im;
-                } else {
-                    const int p = g - T;
-                    D[((2 * p) * 3 + 2) * L + x] = z.re;
-                    if (2 * p + 1 < T) D[((2 * p + 1) * 3 + 2) * L + x] = z.im;
-                }
-            }
-            __syncthreads();
-        }
+// Per-cell epilogue of the row-inverse pass (shared by the generic and the
+// register-FFT kernels): local terms, demag from dfield(r, i, c), torque,
+// stage torque store, RK error norm and FP64 block reductions.
+template <typename R, typename DF>
+__device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& spec, StepState* st, int blk, int T,
+                                             bool do_fft, DF dfield, double* sm_red) {
+    const int nx = F.nx, ny = F.ny, n = nx * ny;
+    const int j0 = blk * T;
+    const int cur = st->cur;
         const R* __restrict__ msb = mbuf<R>(F, spec.m_in, cur);
         R* __restrict__ kout = spec.k_out != KB_NONE ? kbuf<R>(F, spec.k_out, cur) : nullptr;
         R* __restrict__ bout = reinterpret_cast<R*>(F.bout);
@@ -494,9 +439,9 @@ __global__ void __launch_bounds__(256) k_row_inverse(const FilmDev* __restrict__
             if (spec.rhs == RHS_ENERGY) {
                 double bd[3] = {0.0, 0.0, 0.0};
                 if (do_fft) {
-                    bd[0] = (double)D[(r * 3 + 0) * L + i];
-                    bd[1] = (double)D[(r * 3 + 1) * L + i];
-                    bd[2] = (double)D[(r * 3 + 2) * L + i];
+                    bd[0] = (double)dfield(r, i, 0);
+                    bd[1] = (double)dfield(r, i, 1);
+                    bd[2] = (double)dfield(r, i, 2);
                 }
                 energy_terms<R>(F, msb, i, j, bd, do_fft, red);
                 continue;
@@ -507,9 +452,9 @@ __global__ void __launch_bounds__(256) k_row_inverse(const FilmDev* __restrict__
                 b[0] = (R)0; b[1] = (R)0; b[2] = (R)0;
             }
             if (do_fft) {
-                b[0] += D[(r * 3 + 0) * L + i];
-                b[1] += D[(r * 3 + 1) * L + i];
-                b[2] += D[(r * 3 + 2) * L + i];
+                b[0] += dfield(r, i, 0);
+                b[1] += dfield(r, i, 1);
+                b[2] += dfield(r, i, 2);
             }
             if (spec.rhs == RHS_FIELD) {
                 bout[idx] = b[0]; bout[n + idx] = b[1]; bout[2 * n + idx] = b[2];
@@ -620,10 +565,77 @@ __global__ void __launch_bounds__(256) k_row_inverse(const FilmDev* __restrict__
         if (spec.reduce) {
             block_reduce(red, sm_red);
             if (threadIdx.x == 0) {
-                double* dst = F.red_part + (size_t)w.blk * RED_NSLOT;
+                double* dst = F.red_part + (size_t)blk * RED_NSLOT;
                 for (int s = 0; s < RED_NSLOT; ++s) dst[s] = red[s];
             }
         }
+}
+
+// ---------------------------------------------------------------------------
+// Pass 3: C2R along x + local terms + torque + error norm + reductions.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256) k_row_inverse(const FilmDev* __restrict__ films,
+                                                     const WorkItem* __restrict__ items, int nitems, EvalSpec spec) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double sm_red[32 * RED_NSLOT];
+    cx<R>* sm = reinterpret_cast<cx<R>*>(smem_raw);
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const WorkItem w = items[it];
+        const FilmDev& F = films[w.film];
+        StepState* st = F.st;
+        if (!st->active) continue;
+        if (spec.skip_if_fsal && st->fsal_valid) continue;
+        const int nx = F.nx, ny = F.ny, T = F.rows_per_block;
+        const int j0 = w.blk * T;
+        const int L = nx, K1 = nx + 1, L2 = 2 * nx;
+        const int G = T + (T + 1) / 2, P = (T + 1) / 2;
+        const bool do_fft = spec.demag && F.demag_mat;
+        const cx<R>* __restrict__ tw = reinterpret_cast<const cx<R>*>(F.tw_row);
+        R* D = nullptr;
+        if (do_fft) {
+            const cx<R>* __restrict__ X = reinterpret_cast<const cx<R>*>(F.X);
+            cx<R>* A = sm;
+            cx<R>* B = sm + 2 * G * L;
+            auto xval = [&](int c, int k, int j) -> cx<R> {
+                if (k <= nx) return X[(c * K1 + k) * ny + j];
+                return conjc(X[(c * K1 + (L2 - k)) * ny + j]);
+            };
+            for (int e = threadIdx.x; e < L2 * T; e += blockDim.x) {
+                const int r = e % T, k = e / T, j = j0 + r;
+                cx<R> z = mkc((R)0, (R)0);
+                if (j < ny) {
+                    cx<R> bx = xval(0, k, j), by = xval(1, k, j);
+                    z = mkc(bx.re - by.im, bx.im + by.re);
+                }
+                A[(2 * r + (k & 1)) * L + (k >> 1)] = z;
+            }
+            for (int e = threadIdx.x; e < L2 * P; e += blockDim.x) {
+                const int p = e % P, k = e / P;
+                const int ja = j0 + 2 * p, jb = j0 + 2 * p + 1;
+                cx<R> za = (ja < ny) ? xval(2, k, ja) : mkc((R)0, (R)0);
+                cx<R> zb = (2 * p + 1 < T && jb < ny) ? xval(2, k, jb) : mkc((R)0, (R)0);
+                A[(2 * (T + p) + (k & 1)) * L + (k >> 1)] = mkc(za.re - zb.im, za.im + zb.re);
+            }
+            __syncthreads();
+            cx<R>* res = fft_smem<R>(A, B, 2 * G, F.plan_row, tw, true);
+            D = reinterpret_cast<R*>(res == A ? B : A);
+            for (int e = threadIdx.x; e < G * L; e += blockDim.x) {
+                const int g = e / L, x = e - g * L;
+                cx<R> z = res[(2 * g) * L + x] + cmulc(res[(2 * g + 1) * L + x], tw[x]);
+                if (g < T) {
+                    D[(g * 3 + 0) * L + x] = z.re;
+                    D[(g * 3 + 1) * L + x] = z.im;
+                } else {
+                    const int p = g - T;
+                    D[((2 * p) * 3 + 2) * L + x] = z.re;
+                    if (2 * p + 1 < T) D[((2 * p + 1) * 3 + 2) * L + x] = z.im;
+                }
+            }
+            __syncthreads();
+        }
+        auto dfield = [&](int r, int i, int c) -> R { return D[(r * 3 + c) * L + i]; };
+        row_epilogue<R>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
         __syncthreads();
     }
 }

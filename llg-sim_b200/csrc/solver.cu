@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -226,6 +227,13 @@ struct EngineBase {
     virtual long long launch_count() = 0;
 };
 
+// LLG_B200_GENERIC_FFT=1 selects the generic shared-memory Stockham kernels
+// even where a register-FFT kernel exists (used to cross-check the two paths).
+static bool force_generic() {
+    const char* e = std::getenv("LLG_B200_GENERIC_FFT");
+    return e && e[0] == '1';
+}
+
 template <typename R>
 struct Engine final : EngineBase {
     int device = 0;
@@ -291,13 +299,17 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
         stream = own_stream;
         CUDA_TRY(cudaMallocHost(&h_state, sizeof(StepState)));
-        const int T = 2;
-        const int G = T + (T + 1) / 2;
         const bool demag = mat.demag != 0;
+        // register-FFT kernels for power-of-two sizes, generic kernels otherwise
+        const FastCfg fc = fast_config<R>(nx, ny);
+        const bool fast = fc.ok && !force_generic();
+        const int T = fast ? fc.T : 2;
+        const int NC = fast ? fc.NC : 1;
+        const int G = T + (T + 1) / 2;
         size_t smem_row = demag ? 4 * (size_t)G * nx * sizeof(cx<R>) : 0;
         size_t smem_col = demag ? 12 * (size_t)ny * sizeof(cx<R>) : 0;
         const size_t smem_max = 227 * 1024;
-        if (smem_row > smem_max || smem_col > smem_max)
+        if (!fast && (smem_row > smem_max || smem_col > smem_max))
             return set_error(LLG_ERR_INVALID, "grid %dx%d exceeds the in-shared-memory FFT limit for this precision",
                              nx, ny);
         int rc;
@@ -357,6 +369,15 @@ struct Engine final : EngineBase {
             CUDA_TRY(launch_twiddles(tw_col, 2 * ny, sizeof(R) == 8, stream));
             F.tw_row = tw_row;
             F.tw_col = tw_col;
+            if (fast) {
+                void* twp_row;
+                void* twp_col;
+                if ((rc = dalloc(&twp_row, sizeof(cx<R>) * (size_t)std::max(fc.twp_row_size, 1)))) return rc;
+                if ((rc = dalloc(&twp_col, sizeof(cx<R>) * (size_t)std::max(fc.twp_col_size, 1)))) return rc;
+                CUDA_TRY(build_pass_tables<R>(twp_row, nx, twp_col, ny, stream));
+                F.twp_row = twp_row;
+                F.twp_col = twp_col;
+            }
             if ((rc = dalloc(&F.X, sizeof(cx<R>) * 3 * (size_t)(nx + 1) * ny))) return rc;
             void* kh;
             if ((rc = dalloc(&kh, sizeof(r4<R>) * (size_t)(nx + 1) * (ny + 1)))) return rc;
@@ -366,9 +387,10 @@ struct Engine final : EngineBase {
         }
         if ((rc = dalloc(&d_film, sizeof(FilmDev)))) return rc;
         CUDA_TRY(cudaMemcpyAsync(d_film, &F, sizeof(FilmDev), cudaMemcpyHostToDevice, stream));
-        std::vector<WorkItem> rows(F.nblk), cols(nx + 1);
+        const int ncol_blk = (nx + 1 + NC - 1) / NC;
+        std::vector<WorkItem> rows(F.nblk), cols(ncol_blk);
         for (int b = 0; b < F.nblk; ++b) rows[b] = WorkItem{0, b};
-        for (int b = 0; b <= nx; ++b) cols[b] = WorkItem{0, b};
+        for (int b = 0; b < ncol_blk; ++b) cols[b] = WorkItem{0, b};
         if ((rc = dalloc(&d_row_items, sizeof(WorkItem) * rows.size()))) return rc;
         if ((rc = dalloc(&d_col_items, sizeof(WorkItem) * cols.size()))) return rc;
         CUDA_TRY(cudaMemcpyAsync(d_row_items, rows.data(), sizeof(WorkItem) * rows.size(), cudaMemcpyHostToDevice,
@@ -379,13 +401,17 @@ struct Engine final : EngineBase {
         geom.row_items = d_row_items;
         geom.n_row_items = F.nblk;
         geom.col_items = d_col_items;
-        geom.n_col_items = nx + 1;
+        geom.n_col_items = ncol_blk;
         geom.smem_row = smem_row;
         geom.smem_col = smem_col;
         geom.grid_row = F.nblk;
-        geom.grid_col = nx + 1;
+        geom.grid_col = ncol_blk;
         geom.any_demag = demag;
-        CUDA_TRY(prepare_eval_kernels<R>(smem_row, smem_col));
+        geom.fast_row = fast ? nx : 0;
+        geom.fast_col = fast ? ny : 0;
+        geom.row_threads = fast ? fc.row_threads : 256;
+        geom.col_threads = fast ? fc.col_threads : 256;
+        CUDA_TRY(prepare_eval_kernels<R>(fast ? 0 : smem_row, fast ? 0 : smem_col));
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
     }

@@ -178,3 +178,45 @@ def test_mean_m_and_state_roundtrip(gpu, orc):
     g.set_state(m)
     assert np.array_equal(g.get_state(), m)
     assert np.allclose(g.mean_m(), m.mean(axis=0), atol=1e-14)
+
+
+FAST_SHAPES = [(16, 16), (32, 64), (64, 128), (128, 256), (256, 32), (512, 16), (1024, 64), (2048, 16), (16, 2048),
+               (64, 1024)]
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("nx,ny", FAST_SHAPES)
+def test_register_fft_path_matches_oracle(orc, gpu, nx, ny, prec):
+    """Power-of-two sizes run the register-FFT kernels; fields must match the oracle."""
+    if prec == 1 and max(nx, ny) > 1024:
+        pytest.skip("FP64 in-shared-memory transforms are limited to 1024")
+    c = case(nx, ny, dmi=2e-3, k_u=1e5)
+    o = oracle_solver(orc, c)
+    g = gpu_solver(gpu, c, prec)
+    m = random_m(orc, nx * ny, 21 + nx + ny)
+    g.set_state(m)
+    bext = (0.01, 0.0, -0.02)
+    p = gpu.LLGParams(GAMMA, 0.1, 1e-13, bext)
+    assert rel_err(g.build_h_eff(p, 2), o.build_h_eff(m, bext, 2)) <= TOL[prec]
+    assert rel_err(g.compute_demag_field(), o.demag_field(m)) <= TOL[prec]
+
+
+@pytest.mark.parametrize("nx,ny", [(256, 256), (128, 64), (1024, 32)])
+def test_register_fft_matches_generic_kernels(orc, gpu, nx, ny, monkeypatch):
+    c = case(nx, ny)
+    m = random_m(orc, nx * ny, 5)
+    fast = gpu_solver(gpu, c, gpu.FP64)
+    monkeypatch.setenv("LLG_B200_GENERIC_FFT", "1")
+    gen = gpu_solver(gpu, c, gpu.FP64)
+    monkeypatch.delenv("LLG_B200_GENERIC_FFT")
+    fast.set_state(m)
+    gen.set_state(m)
+    p = gpu.LLGParams(GAMMA, 0.02, 1e-13, (0.0, 0.01, 0.0))
+    assert rel_err(fast.build_h_eff(p, 2), gen.build_h_eff(p, 2)) <= 1e-12
+    for _ in range(3):
+        rf = fast.step_rk45(p, 2, 1e-5, 0.8, 1e-19, 1e-11)
+        p.dt = rf[2]
+        rg = gen.step_rk45(p, 2, 1e-5, 0.8, 1e-19, 1e-11)
+        assert rf[1] == rg[1]
+        p.dt = rf[2]
+    assert np.abs(fast.get_state() - gen.get_state()).max() <= 1e-12
