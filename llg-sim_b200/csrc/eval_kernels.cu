@@ -4,6 +4,8 @@
 #include "build_api.h"
 #include "fast_kernels.cuh"
 
+#include <algorithm>
+
 namespace llg {
 
 namespace {
@@ -24,6 +26,12 @@ bool dispatch_L(int L, F&& f) {
 }
 
 constexpr size_t kSmemMax = 227 * 1024;
+
+// Intermediate RK stages need only the torque: no reductions, error norm or
+// field output.
+bool lean_epilogue(const EvalSpec& e) {
+    return e.err == ERR_NONE && !e.reduce && e.local && (e.rhs == RHS_LLG || e.rhs == RHS_RELAX);
+}
 
 }  // namespace
 
@@ -84,7 +92,9 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
         if (RowCfg<R, L>::SMEM <= kSmemMax) {
             cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_row_inverse_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_row_inverse_fast<R, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)RowCfg<R, L>::SMEM);
+            cudaFuncSetAttribute(k_row_inverse_fast<R, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
         }
         if (ColCfg<R, L>::SMEM <= kSmemMax)
@@ -105,8 +115,11 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
                     if (which == 0)
                         k_row_forward_fast<R, L><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
                             g.films, g.row_items, g.n_row_items, spec);
+                    else if (lean_epilogue(spec))
+                        k_row_inverse_fast<R, L, true><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                            g.films, g.row_items, g.n_row_items, spec);
                     else
-                        k_row_inverse_fast<R, L><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                        k_row_inverse_fast<R, L, false><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
                             g.films, g.row_items, g.n_row_items, spec);
                 }
             });
@@ -141,6 +154,36 @@ cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t 
     return launch_one<R>(2, spec, g, s);
 }
 
+template <typename R>
+void fast_occupancy(int nx, int ny, int* row_blocks_per_sm, int* col_blocks_per_sm) {
+    *row_blocks_per_sm = 1;
+    *col_blocks_per_sm = 1;
+    dispatch_L<R>(nx, [&](auto LC) {
+        constexpr int L = decltype(LC)::value;
+        if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
+            int a = 1, b = 1, c = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_row_forward_fast<R, L>, RowCfg<R, L>::THREADS,
+                                                          RowCfg<R, L>::SMEM);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_row_inverse_fast<R, L, false>, RowCfg<R, L>::THREADS,
+                                                          RowCfg<R, L>::SMEM);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_row_inverse_fast<R, L, true>, RowCfg<R, L>::THREADS,
+                                                          RowCfg<R, L>::SMEM);
+            *row_blocks_per_sm = std::max(1, std::min(a, std::min(b, c)));
+        }
+    });
+    dispatch_L<R>(ny, [&](auto LC) {
+        constexpr int L = decltype(LC)::value;
+        if constexpr (ColCfg<R, L>::SMEM <= kSmemMax) {
+            int a = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L>, ColCfg<R, L>::THREADS,
+                                                          ColCfg<R, L>::SMEM);
+            *col_blocks_per_sm = std::max(1, a);
+        }
+    });
+}
+
+template void fast_occupancy<float>(int, int, int*, int*);
+template void fast_occupancy<double>(int, int, int*, int*);
 template FastCfg fast_config<float>(int, int);
 template FastCfg fast_config<double>(int, int);
 template cudaError_t build_pass_tables<float>(void*, int, void*, int, cudaStream_t);

@@ -202,26 +202,23 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
         for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FF::out_index(t, i))] = v[i];
         __syncthreads();
         {
-            const r4<R>* __restrict__ Kh = reinterpret_cast<const r4<R>*>(F.Khat) + (size_t)(valid ? kx : 0) * (ny + 1);
+            const r4<R>* __restrict__ Kp =
+                reinterpret_cast<const r4<R>*>(F.Kpar) + ((size_t)(valid ? kx : 0) * 2 + par) * ny;
             const cx<R>* sx = buf + (6 * cl + 0 + par) * BUF;
             const cx<R>* sy = buf + (6 * cl + 2 + par) * BUF;
             const cx<R>* sz = buf + (6 * cl + 4 + par) * BUF;
 #pragma unroll
             for (int r = 0; r < E; ++r) {
                 const int kk = t + G * r;
-                const int ky = 2 * kk + par;
-                const int kyf = ky <= ny ? ky : 2 * ny - ky;
-                const r4<R> K = Kh[kyf];
+                const r4<R> K = Kp[kk];
                 const int pi = padi<E>(kk);
                 cx<R> out;
                 if (comp == 0) {
-                    const R kxy = ky <= ny ? K.y : -K.y;
                     const cx<R> Mx = sx[pi], My = sy[pi];
-                    out = mkc(K.x * Mx.re + kxy * My.re, K.x * Mx.im + kxy * My.im);
+                    out = mkc(K.x * Mx.re + K.y * My.re, K.x * Mx.im + K.y * My.im);
                 } else if (comp == 1) {
-                    const R kxy = ky <= ny ? K.y : -K.y;
                     const cx<R> Mx = sx[pi], My = sy[pi];
-                    out = mkc(kxy * Mx.re + K.z * My.re, kxy * Mx.im + K.z * My.im);
+                    out = mkc(K.y * Mx.re + K.z * My.re, K.y * Mx.im + K.z * My.im);
                 } else {
                     const cx<R> Mz = sz[pi];
                     out = mkc(K.w * Mz.re, K.w * Mz.im);
@@ -250,7 +247,7 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
 }
 
 // ---------------------------------------------------------------------------
-template <typename R, int L>
+template <typename R, int L, bool LEAN>
 __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_inverse_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
                                                                             int nitems, EvalSpec spec) {
@@ -282,29 +279,35 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_inverse_fast(cons
         if (do_fft) {
             const cx<R>* __restrict__ X = reinterpret_cast<const cx<R>*>(F.X);
             constexpr int K1 = L + 1, L2 = 2 * L;
-            auto xval = [&](int c, int k, int j) -> cx<R> {
-                if (k <= L) return X[(size_t)(c * K1 + k) * ny + j];
-                return conjc(X[(size_t)(c * K1 + (L2 - k)) * ny + j]);
+            // stage this block's rows of the spectrum, [c][k][r], with contiguous
+            // T-row chunks per (c, k) (the signal buffers are free here)
+            cx<R>* stg = buf;
+            for (int e = tid; e < 3 * K1 * T; e += C::THREADS) {
+                const int r = e % T, ck = e / T;
+                const int j = j0 + r;
+                stg[e] = j < ny ? X[(size_t)ck * ny + j] : mkc((R)0, (R)0);
+            }
+            __syncthreads();
+            auto xval = [&](int c, int k, int r) -> cx<R> {
+                if (k <= L) return stg[(c * K1 + k) * T + r];
+                return conjc(stg[(c * K1 + (L2 - k)) * T + r]);
             };
             cx<R> v[E];
 #pragma unroll
             for (int r = 0; r < E; ++r) {
                 const int k = 2 * (t + G * r) + par;
-                cx<R> z = mkc((R)0, (R)0);
+                cx<R> z;
                 if (g < T) {
-                    const int j = j0 + g;
-                    if (j < ny) {
-                        const cx<R> bx = xval(0, k, j), by = xval(1, k, j);
-                        z = mkc(bx.re - by.im, bx.im + by.re);
-                    }
+                    const cx<R> bx = xval(0, k, g), by = xval(1, k, g);
+                    z = mkc(bx.re - by.im, bx.im + by.re);
                 } else {
-                    const int ja = j0 + 2 * (g - T), jb = ja + 1;
-                    const cx<R> za = ja < ny ? xval(2, k, ja) : mkc((R)0, (R)0);
-                    const cx<R> zb = jb < ny ? xval(2, k, jb) : mkc((R)0, (R)0);
+                    const int ra = 2 * (g - T);
+                    const cx<R> za = xval(2, k, ra), zb = xval(2, k, ra + 1);
                     z = mkc(za.re - zb.im, za.im + zb.re);
                 }
                 v[r] = z;
             }
+            __syncthreads();
             FI::run(v, t, buf + s * BUF, twp);
             __syncthreads();
             if (par) {
@@ -332,7 +335,8 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_inverse_fast(cons
             const cx<R> z = buf[(2 * (T + r / 2)) * BUF + padi<E>(i)];
             return (r & 1) ? z.im : z.re;
         };
-        row_epilogue<R>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
+        if constexpr (LEAN) row_epilogue_lean<R>(F, spec, st, w.blk, T, do_fft, dfield);
+        else row_epilogue<R>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
         __syncthreads();
     }
 }

@@ -571,6 +571,46 @@ __device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& s
         }
 }
 
+// Epilogue of an intermediate RK stage: local terms + demag + torque only.
+template <typename R, typename DF>
+__device__ __forceinline__ void row_epilogue_lean(const FilmDev& F, const EvalSpec& spec, const StepState* st, int blk,
+                                                  int T, bool do_fft, DF dfield) {
+    const int nx = F.nx, ny = F.ny, n = nx * ny;
+    const int j0 = blk * T;
+    const int cur = st->cur;
+    const R* __restrict__ msb = mbuf<R>(F, spec.m_in, cur);
+    R* __restrict__ kout = kbuf<R>(F, spec.k_out, cur);
+    const R gam = (R)F.gamma, alp = (R)F.alpha;
+    const R denom = (R)1 + alp * alp;
+    const R pref = spec.rhs == RHS_LLG ? -gam / denom : -gam * alp / denom;
+    const R c1 = spec.rhs == RHS_LLG ? (R)1 : (R)0;
+    const R c2 = spec.rhs == RHS_LLG ? alp : (R)1;
+    for (int e = threadIdx.x; e < T * nx; e += blockDim.x) {
+        const int r = e / nx, i = e - r * nx, j = j0 + r;
+        if (j >= ny) continue;
+        const int idx = j * nx + i;
+        R mc[3];
+        ld3(msb, n, idx, mc);
+        R b[3];
+        local_field<R>(F, msb, i, j, spec.dmi != 0, mc, b);
+        if (do_fft) {
+            b[0] += dfield(r, i, 0);
+            b[1] += dfield(r, i, 1);
+            b[2] += dfield(r, i, 2);
+        }
+        // llg_rhs (llg.rs:20-32) / llg_rhs_relax (llg.rs:38-50)
+        const R t0 = mc[1] * b[2] - mc[2] * b[1];
+        const R t1 = mc[2] * b[0] - mc[0] * b[2];
+        const R t2 = mc[0] * b[1] - mc[1] * b[0];
+        const R u0 = mc[1] * t2 - mc[2] * t1;
+        const R u1 = mc[2] * t0 - mc[0] * t2;
+        const R u2 = mc[0] * t1 - mc[1] * t0;
+        kout[idx] = pref * (c1 * t0 + c2 * u0);
+        kout[n + idx] = pref * (c1 * t1 + c2 * u1);
+        kout[2 * n + idx] = pref * (c1 * t2 + c2 * u2);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Pass 3: C2R along x + local terms + torque + error norm + reductions.
 // ---------------------------------------------------------------------------

@@ -5,6 +5,7 @@
 // FP64 step controller, all reading their dynamic state (dt, buffer parity,
 // activity) from device memory so that an attempt — or a run of attempts — is
 // captured once as a CUDA graph and replayed without host round trips.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -384,6 +385,12 @@ struct Engine final : EngineBase {
             F.Khat = kh;
             if ((rc = dalloc(&d_k64, sizeof(double) * 4 * (size_t)(nx + 1) * (ny + 1)))) return rc;
             CUDA_TRY(build_demag_kernel(nx, ny, g->dx, g->dy, g->dz, sizeof(R) == 8, kh, d_k64, stream));
+            if (fast) {
+                void* kp;
+                if ((rc = dalloc(&kp, sizeof(r4<R>) * (size_t)(nx + 1) * 2 * ny))) return rc;
+                CUDA_TRY(build_kernel_parity(nx, ny, sizeof(R) == 8, kh, kp, stream));
+                F.Kpar = kp;
+            }
         }
         if ((rc = dalloc(&d_film, sizeof(FilmDev)))) return rc;
         CUDA_TRY(cudaMemcpyAsync(d_film, &F, sizeof(FilmDev), cudaMemcpyHostToDevice, stream));
@@ -412,9 +419,49 @@ struct Engine final : EngineBase {
         geom.row_threads = fast ? fc.row_threads : 256;
         geom.col_threads = fast ? fc.col_threads : 256;
         CUDA_TRY(prepare_eval_kernels<R>(fast ? 0 : smem_row, fast ? 0 : smem_col));
+        if (fast) {
+            // persistent grids: one wave of resident blocks looping over the work
+            // items, so the twiddle tables are loaded once per block
+            int nsm = 148, rb = 1, cb = 1;
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            fast_occupancy<R>(nx, ny, &rb, &cb);
+            geom.grid_row = std::min(F.nblk, nsm * rb);
+            geom.grid_col = std::min(ncol_blk, nsm * cb);
+        }
+        if (demag) set_l2_window();
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
     }
+
+    // Keep the spectrum scratch (written by the row pass, read by the column
+    // pass, read again by the row-inverse pass) resident in L2 across the
+    // passes of an evaluation.  The persisting carve-out is a property of this
+    // process's context only.
+    void set_l2_window() {
+        int dev = device;
+        int max_persist = 0, max_window = 0;
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev);
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+        if (max_persist <= 0 || max_window <= 0 || !fh.X) return;
+        const size_t xbytes = sizeof(cx<R>) * 3 * (size_t)(fh.nx + 1) * fh.ny;
+        size_t want = std::min<size_t>(xbytes, (size_t)max_persist);
+        if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        cudaStreamAttrValue attr{};
+        attr.accessPolicyWindow.base_ptr = fh.X;
+        attr.accessPolicyWindow.num_bytes = std::min<size_t>(xbytes, (size_t)max_window);
+        attr.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)want / (double)attr.accessPolicyWindow.num_bytes);
+        attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        l2_attr = attr;
+        l2_window = true;
+        if (cudaStreamSetAttribute(own_stream, cudaStreamAttributeAccessPolicyWindow, &attr) != cudaSuccess)
+            cudaGetLastError();
+    }
+    bool l2_window = false;
+    cudaStreamAttrValue l2_attr{};
 
     int upload_film() {
         CUDA_TRY(cudaMemcpyAsync(d_film, &fh, sizeof(FilmDev), cudaMemcpyHostToDevice, stream));
@@ -424,6 +471,8 @@ struct Engine final : EngineBase {
     int set_stream(cudaStream_t s) override {
         CUDA_TRY(cudaStreamSynchronize(stream));
         stream = s ? s : own_stream;
+        if (l2_window && cudaStreamSetAttribute(stream, cudaStreamAttributeAccessPolicyWindow, &l2_attr) != cudaSuccess)
+            cudaGetLastError();
         return LLG_OK;
     }
     int sync() override {
