@@ -186,6 +186,29 @@ int llg_demag_kernel_kspace(llg_solver* s, double* out /* 4*(nx+1)*(ny+1) */);
 int llg_profile_stage(llg_solver* s, const llg_params* params, int32_t field_mask, int32_t reps, double* ms3);
 int llg_solver_launch_count(llg_solver* s, int64_t* out);
 
+/* ---------------- demag field without device allocation ----------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory at the point of use — a host framework whose pool owns every device
+ * allocation, a real-time loop that cannot pay allocation latency, code where
+ * cudaMalloc is not permitted.  Computes the demag field of one nx x ny film
+ * (the field of llg_compute_demag_field) on the current CUDA device and calls
+ * no cudaMalloc/cudaFree or allocating library routine.
+ *   m             device, FP32 SoA [3][ny][nx] magnetisation (unit vectors)
+ *   ms            saturation magnetisation (A/m)
+ *   kernel_planes device, FP64 [4][ny+1][nx+1]: the planes llg_demag_kernel_kspace returns
+ *   b_out         device, FP32 SoA [3][ny][nx], overwritten with B_demag (T)
+ *   stream        cudaStream_t or NULL; the call is asynchronous on it
+ * Scratch: one static 32 MiB device array per GPU that loads the library,
+ * held until exit; requires 1 <= nx, ny <= 2048 and
+ * 24*(nx+1)*ny + 16*(nx+ny) <= 32 MiB (e.g. 1024 x 1024), else LLG_ERR_INVALID.
+ * The first call on a device looks up the array's device address and opts the
+ * kernels into large shared memory; make that first call before any stream
+ * capture.  Every call shares the array (no state carries over: each call
+ * rewrites all of it before reading), so calls that overlap on the GPU — on
+ * different streams or from different threads — race; serialise them. */
+int llg_demag_field_noalloc(int64_t nx, int64_t ny, double ms, const float* m, const double* kernel_planes,
+                            float* b_out, void* stream);
+
 /* ---------------- initial states (initial_states.rs) ---------------- */
 void llg_init_random(int64_t n, uint64_t seed, double* m_aos);                   /* :59-68 */
 void llg_init_uniform_with_noise(int64_t n, const double dir[3], double noise,  /* :43-56 */

@@ -3,6 +3,9 @@
 #include <cuda_runtime.h>
 #include "types.cuh"
 
+// Sets the calling thread's message returned by llg_last_error().
+void llg_set_error_message(const char* msg);
+
 namespace llg {
 
 FftPlan make_plan(int L);

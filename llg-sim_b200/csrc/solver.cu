@@ -1172,6 +1172,9 @@ int bind(llg_solver* s) {
 }
 }  // namespace
 
+// Lets other translation units report through llg_last_error().
+void llg_set_error_message(const char* msg) { llg::g_last_error = msg ? msg : ""; }
+
 extern "C" {
 
 int llg_abi_version(void) { return LLG_B200_ABI_VERSION; }

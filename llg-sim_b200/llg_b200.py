@@ -135,6 +135,7 @@ def lib():
             "llg_demag_kernel_kspace": (C.c_int, [vp, dp]),
             "llg_profile_stage": (C.c_int, [vp, P(_Params), i32, i32, dp]),
             "llg_solver_launch_count": (C.c_int, [vp, P(i64)]),
+            "llg_demag_field_noalloc": (C.c_int, [i64, i64, C.c_double, vp, vp, vp, vp]),
             "llg_init_random": (None, [i64, C.c_uint64, dp]),
             "llg_init_uniform_with_noise": (None, [i64, dp, C.c_double, C.c_uint64, dp]),
         }
@@ -349,6 +350,13 @@ class Solver:
         out = np.empty(4 * (self.grid.nx + 1) * (self.grid.ny + 1))
         _check(lib().llg_demag_kernel_kspace(self.h, _dp(out)))
         return out.reshape(4, self.grid.ny + 1, self.grid.nx + 1)
+
+
+def demag_field_noalloc(nx, ny, ms, m_dev_ptr, kernel_planes_dev_ptr, b_dev_ptr, stream_ptr=0):
+    """Demag field with no device allocation (raw device pointers, see include/llg_b200.h)."""
+    _check(lib().llg_demag_field_noalloc(int(nx), int(ny), float(ms), C.c_void_p(m_dev_ptr),
+                                         C.c_void_p(kernel_planes_dev_ptr), C.c_void_p(b_dev_ptr),
+                                         C.c_void_p(stream_ptr)))
 
 
 def init_random(n, seed):
