@@ -162,7 +162,9 @@ int llg_run_rk45(llg_solver* s, llg_params* params, int32_t field_mask, double m
                  double dt_min, double dt_max, int64_t n_accepted, double t_end, int64_t max_attempts,
                  int64_t* accepted_out, int64_t* rejected_out, double* t_advanced);
 
-/* relax_with_report (relax.rs:334-768).  settings->max_err is written back. */
+/* relax_with_report (relax.rs:334-768), run by a device-side controller that
+ * restates its two phases, torque checks and MaxErr tightening per film;
+ * settings->max_err is written back. */
 int llg_relax(llg_solver* s, llg_params* params, int32_t field_mask, llg_relax_settings* settings,
               llg_relax_report* report);
 void llg_default_relax_settings(llg_relax_settings* st); /* impl Default, relax.rs:107-141 */
@@ -177,6 +179,37 @@ int llg_torque_metric(llg_solver* s, const llg_params* params, int32_t field_mas
  * K = mu0 * N on kx in [0,nx], ky in [0,ny], as FP64, without the 1/(px*py)
  * scaling (compare with the real part of Demag2D::kxx.. at those indices). */
 int llg_demag_kernel_kspace(llg_solver* s, double* out /* 4*(nx+1)*(ny+1) */);
+
+/* ---------------- batches of independent films ----------------
+ * Many films (sizes, materials, masks may differ) advance together: every
+ * pass of an evaluation is one launch over the work items of all films, each
+ * film with its own dt, acceptance and FSAL state (the per-film semantics of
+ * the single-film calls above, llg.rs:278-436 / 795-1026).  When all films
+ * share one power-of-two shape the register-FFT kernels are used, otherwise the
+ * generic shared-memory ones.  Films with identical grids share the demag
+ * operator (get_demag_operator keys it by grid, demag_fft_uniform.rs:86).
+ * Arrays of params / results are indexed by film; masks is nullable and may
+ * hold null entries. */
+typedef struct llg_batch llg_batch;
+int llg_batch_create(llg_ctx* ctx, int32_t nfilms, const llg_grid* grids, const llg_material* mats,
+                     int32_t precision, const uint8_t* const* masks, llg_batch** out);
+int llg_batch_destroy(llg_batch* b);
+int llg_batch_set_stream(llg_batch* b, void* stream);
+int llg_batch_set_state(llg_batch* b, int32_t film, const double* m_aos);
+int llg_batch_get_state(llg_batch* b, int32_t film, double* m_aos);
+int llg_batch_mean_m(llg_batch* b, double* out /* 3*nfilms */);
+/* one RK45 attempt for every film (step_llg_rk45_recompute_field_masked_adaptive, llg.rs:795) */
+int llg_batch_step_rk45(llg_batch* b, llg_params* params, int32_t field_mask, double max_err, double headroom,
+                        double dt_min, double dt_max, double* eps, int32_t* accepted, double* dt_used);
+/* device-resident RK45 for every film until n_accepted more steps or simulated time t_end each */
+int llg_batch_run_rk45(llg_batch* b, llg_params* params, int32_t field_mask, double max_err, double headroom,
+                       double dt_min, double dt_max, int64_t n_accepted, double t_end, int64_t max_attempts,
+                       int64_t* accepted, int64_t* rejected, double* t);
+/* relax_with_report (relax.rs:334-768) for every film, driven by a device-side controller */
+int llg_batch_relax(llg_batch* b, llg_params* params, int32_t field_mask, const llg_relax_settings* settings,
+                    llg_relax_report* reports);
+int llg_batch_compute_energy(llg_batch* b, const double* b_ext /* 3*nfilms */, llg_energy_breakdown* out);
+int llg_batch_launch_count(llg_batch* b, int64_t* out);
 
 /* ---------------- instrumentation (no reference counterpart) ----------------
  * llg_profile_stage: CUDA-event timing of the three passes of one RK45 stage

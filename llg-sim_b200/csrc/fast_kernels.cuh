@@ -63,8 +63,7 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_forward_fast(cons
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
         const StepState* st = F.st;
-        if (!st->active) continue;
-        if (spec.skip_if_fsal && st->fsal_valid) continue;
+        if (skip_item(spec, st)) continue;
         const bool do_fft = spec.demag && F.demag_mat;
         if (do_fft && !tables) {
             load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_row), TwTab<R, L>::size, pre,
@@ -175,8 +174,7 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
         const StepState* st = F.st;
-        if (!st->active) continue;
-        if (spec.skip_if_fsal && st->fsal_valid) continue;
+        if (skip_item(spec, st)) continue;
         if (!(spec.demag && F.demag_mat)) continue;
         if (!tables) {
             load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_col), TwTab<R, L>::size, pre,
@@ -265,8 +263,7 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_inverse_fast(cons
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
         StepState* st = F.st;
-        if (!st->active) continue;
-        if (spec.skip_if_fsal && st->fsal_valid) continue;
+        if (skip_item(spec, st)) continue;
         const bool do_fft = spec.demag && F.demag_mat;
         if (do_fft && !tables) {
             load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_row), TwTab<R, L>::size, pre,

@@ -60,6 +60,15 @@ __device__ __forceinline__ void normalize3(R* v) {
     v[0] *= inv; v[1] *= inv; v[2] *= inv;
 }
 
+// Whether this evaluation skips a film: inactive, FSAL torque still valid, or
+// (request-gated evaluations) the film did not request it.
+__device__ __forceinline__ bool skip_item(const EvalSpec& spec, const StepState* st) {
+    if (!st->active) return true;
+    if (spec.skip_if_fsal && st->fsal_valid) return true;
+    if (spec.req && st->req != spec.req) return true;
+    return false;
+}
+
 __device__ __forceinline__ bool cell_inside(const FilmDev& F, int idx) { return !F.has_mask || F.mask[idx] != 0; }
 
 // Ghost neighbours (exchange.rs:8-35, dmi.rs:19-52, energy.rs:37-64).
@@ -271,8 +280,7 @@ __global__ void __launch_bounds__(256) k_row_forward(const FilmDev* __restrict__
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
         const StepState* st = F.st;
-        if (!st->active) continue;
-        if (spec.skip_if_fsal && st->fsal_valid) continue;
+        if (skip_item(spec, st)) continue;
         const int nx = F.nx, ny = F.ny, n = nx * ny, T = F.rows_per_block;
         const int j0 = w.blk * T;
         const int cur = st->cur;
@@ -370,8 +378,7 @@ __global__ void __launch_bounds__(256) k_column(const FilmDev* __restrict__ film
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
         const StepState* st = F.st;
-        if (!st->active) continue;
-        if (spec.skip_if_fsal && st->fsal_valid) continue;
+        if (skip_item(spec, st)) continue;
         if (!(spec.demag && F.demag_mat)) continue;
         const int nx = F.nx, ny = F.ny, K1 = nx + 1, L = ny;
         const int kx = w.blk;
@@ -624,8 +631,7 @@ __global__ void __launch_bounds__(256) k_row_inverse(const FilmDev* __restrict__
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
         StepState* st = F.st;
-        if (!st->active) continue;
-        if (spec.skip_if_fsal && st->fsal_valid) continue;
+        if (skip_item(spec, st)) continue;
         const int nx = F.nx, ny = F.ny, T = F.rows_per_block;
         const int j0 = w.blk * T;
         const int L = nx, K1 = nx + 1, L2 = 2 * nx;

@@ -1,10 +1,13 @@
 // solver.cu — host driver and C ABI of the B200 LLG path.
 //
-// Engine<R> owns one film's device buffers and runs the integrator attempts as
-// sequences of field evaluations (three kernels each) followed by a one-thread
-// FP64 step controller, all reading their dynamic state (dt, buffer parity,
-// activity) from device memory so that an attempt — or a run of attempts — is
-// captured once as a CUDA graph and replayed without host round trips.
+// Engine<R> owns a set of films (one for llg_solver, many for llg_batch) and
+// runs integrator attempts as sequences of field evaluations (three kernels
+// each, one launch per pass over the work items of every film) followed by a
+// one-thread-per-film FP64 step controller.  Every kernel reads its dynamic
+// state (dt, buffer parity, activity, relax requests) from device memory, so
+// an attempt — or a run of attempts, or relax iterations — is captured once as
+// a CUDA graph and replayed without host round trips; films advance with their
+// own dt and acceptance.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -19,6 +22,7 @@
 #include "../../include/llg_b200.h"
 #include "build_api.h"
 #include "field_kernels.cuh"
+#include "relax_dev.cuh"
 
 namespace llg {
 
@@ -61,23 +65,28 @@ constexpr double B1 = 2.0 / 9.0, B2 = 1.0 / 3.0, B3 = 4.0 / 9.0;
 constexpr double BH1 = 7.0 / 24.0, BH2 = 1.0 / 4.0, BH3 = 1.0 / 3.0, BH4 = 1.0 / 8.0;
 }  // namespace bs3
 
-enum { KIND_RK45 = 1, KIND_RK23 = 2 };
+enum { KIND_RK45 = 1, KIND_RK23 = 2, KIND_RELAX = 3 };
 
+// Shared controller settings; per-film dt and FSAL invalidation come as FilmCtl.
 struct Control {
-    double dt, t_end, max_err, headroom, dt_min, dt_max;
+    double t_end, max_err, headroom, dt_min, dt_max;
     long long target_acc, attempts;
-    int invalidate_fsal;
     int reset_time;
+};
+struct FilmCtl {
+    double dt;
+    int invalidate_fsal;
+    int keep_dt;  // 1: leave StepState::dt as it is
 };
 
 // ---------------------------------------------------------------------------
-// small kernels
+// small kernels (one thread per film unless noted)
 // ---------------------------------------------------------------------------
-__global__ void k_set_control(FilmDev* films, int nfilms, Control c) {
+__global__ void k_set_control(FilmDev* films, int nfilms, Control c, const FilmCtl* __restrict__ fc) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nfilms) return;
     StepState* st = films[f].st;
-    st->dt = c.dt;
+    if (!fc[f].keep_dt) st->dt = fc[f].dt;
     st->t_end = c.t_end;
     st->max_err = c.max_err;
     st->headroom = c.headroom;
@@ -88,7 +97,8 @@ __global__ void k_set_control(FilmDev* films, int nfilms, Control c) {
     st->active = 1;
     st->err_code = 0;
     st->err_bits = 0ull;
-    if (c.invalidate_fsal) st->fsal_valid = 0;
+    st->req = REQ_NONE;
+    if (fc[f].invalidate_fsal) st->fsal_valid = 0;
     if (c.reset_time) st->t = 0.0;
     if (isfinite(c.t_end)) {
         double rem = c.t_end - st->t;
@@ -98,11 +108,12 @@ __global__ void k_set_control(FilmDev* films, int nfilms, Control c) {
 }
 
 // Step-size controller (llg.rs:997-1025 for order 5, llg.rs:401-435 for order 3).
-__global__ void k_controller(FilmDev* films, int nfilms, int order) {
+__global__ void k_controller(FilmDev* films, int nfilms, int order, int req) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nfilms) return;
     StepState* st = films[f].st;
     if (!st->active) return;
+    if (req && st->req != req) return;
     const unsigned long long bits = st->err_bits;
     st->err_bits = 0ull;
     const double err = __longlong_as_double((long long)bits);
@@ -141,11 +152,12 @@ __global__ void k_controller(FilmDev* films, int nfilms, int order) {
     if (stop) st->active = 0;
 }
 
-// Sum the per-block partial reductions in block order (deterministic).
-__global__ void k_finalize(FilmDev* films, int nfilms) {
+// Sum the per-block partial reductions of each film in block order (deterministic).
+__global__ void k_finalize(FilmDev* films, int nfilms, int req) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nfilms) return;
     const FilmDev& F = films[f];
+    if (req && (!F.st->active || F.st->req != req)) return;
     double acc[RED_NSLOT];
     for (int s = 0; s < RED_NSLOT; ++s) acc[s] = 0.0;
     for (int b = 0; b < F.nblk; ++b) {
@@ -155,17 +167,19 @@ __global__ void k_finalize(FilmDev* films, int nfilms) {
     for (int s = 0; s < RED_NSLOT; ++s) F.st->red[s] = acc[s];
 }
 
+// <m> partial sums per row block of every film.
 template <typename R>
-__global__ void k_mean_m(const FilmDev* films) {
+__global__ void k_mean_m(const FilmDev* films, const WorkItem* __restrict__ items, int nitems) {
     __shared__ double sm_red[32 * RED_NSLOT];
-    const FilmDev& F = films[0];
-    const int nx = F.nx, ny = F.ny, n = nx * ny, T = F.rows_per_block;
-    const R* m = mbuf<R>(F, MB_M0, F.st->cur);
-    for (int blk = blockIdx.x; blk < F.nblk; blk += gridDim.x) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const WorkItem w = items[it];
+        const FilmDev& F = films[w.film];
+        const int nx = F.nx, ny = F.ny, n = nx * ny, T = F.rows_per_block;
+        const R* m = mbuf<R>(F, MB_M0, F.st->cur);
         double red[RED_NSLOT];
         for (int s = 0; s < RED_NSLOT; ++s) red[s] = 0.0;
         for (int e = threadIdx.x; e < T * nx; e += blockDim.x) {
-            int j = blk * T + e / nx, i = e % nx;
+            int j = w.blk * T + e / nx, i = e % nx;
             if (j >= ny) continue;
             int idx = j * nx + i;
             red[RED_MX] += (double)m[idx];
@@ -174,14 +188,14 @@ __global__ void k_mean_m(const FilmDev* films) {
         }
         block_reduce(red, sm_red);
         if (threadIdx.x == 0)
-            for (int s = 0; s < RED_NSLOT; ++s) F.red_part[(size_t)blk * RED_NSLOT + s] = red[s];
+            for (int s = 0; s < RED_NSLOT; ++s) F.red_part[(size_t)w.blk * RED_NSLOT + s] = red[s];
         __syncthreads();
     }
 }
 
 template <typename R>
-__global__ void k_aos_to_soa(const FilmDev* films, const double* __restrict__ src) {
-    const FilmDev& F = films[0];
+__global__ void k_aos_to_soa(const FilmDev* films, int film, const double* __restrict__ src) {
+    const FilmDev& F = films[film];
     const int n = F.nx * F.ny;
     R* dst = mbuf<R>(F, MB_M0, F.st->cur);
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
@@ -192,8 +206,8 @@ __global__ void k_aos_to_soa(const FilmDev* films, const double* __restrict__ sr
 }
 
 template <typename R>
-__global__ void k_soa_to_aos(const FilmDev* films, int which, double* __restrict__ dst) {
-    const FilmDev& F = films[0];
+__global__ void k_soa_to_aos(const FilmDev* films, int film, int which, double* __restrict__ dst) {
+    const FilmDev& F = films[film];
     const int n = F.nx * F.ny;
     const R* src = which == 0 ? mbuf<R>(F, MB_M0, F.st->cur) : reinterpret_cast<const R*>(F.bout);
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
@@ -208,22 +222,24 @@ __global__ void k_soa_to_aos(const FilmDev* films, int which, double* __restrict
 // ---------------------------------------------------------------------------
 struct EngineBase {
     virtual ~EngineBase() {}
+    virtual int nfilms() const = 0;
+    virtual int64_t cells(int f) const = 0;
     virtual int set_stream(cudaStream_t s) = 0;
     virtual int sync() = 0;
-    virtual int set_state(const double* m) = 0;
-    virtual int get_state(double* m) = 0;
-    virtual int mean_m(double* out3) = 0;
-    virtual int build_h_eff(const llg_params* p, int fmask, double* b) = 0;
-    virtual int demag_field(double* b) = 0;
+    virtual int set_state(int f, const double* m) = 0;
+    virtual int get_state(int f, double* m) = 0;
+    virtual int mean_m(double* out3n) = 0;
+    virtual int build_h_eff(int f, const llg_params* p, int fmask, double* b) = 0;
+    virtual int demag_field(int f, double* b) = 0;
     virtual int step(int kind, llg_params* p, int fmask, double max_err, double headroom, double dt_min,
                      double dt_max, double* eps, int32_t* acc, double* dtu) = 0;
     virtual int run(int kind, llg_params* p, int fmask, double max_err, double headroom, double dt_min, double dt_max,
                     int64_t n_acc, double t_end, int64_t max_attempts, int64_t* acc_out, int64_t* rej_out,
                     double* t_adv) = 0;
-    virtual int relax(llg_params* p, int fmask, llg_relax_settings* st, llg_relax_report* rep) = 0;
-    virtual int energy(const double* bext, llg_energy_breakdown* out) = 0;
+    virtual int relax(llg_params* p, int fmask, const llg_relax_settings* st, llg_relax_report* rep) = 0;
+    virtual int energy(const double* bext3n, llg_energy_breakdown* out) = 0;
     virtual int torque_metric(const llg_params* p, int fmask, int metric, double* out) = 0;
-    virtual int kernel_kspace(double* out) = 0;
+    virtual int kernel_kspace(int f, double* out) = 0;
     virtual int profile_stage(const llg_params* p, int fmask, int reps, double* ms3) = 0;
     virtual long long launch_count() = 0;
 };
@@ -240,43 +256,48 @@ struct Engine final : EngineBase {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
-    llg_grid grid{};
-    llg_material mat{};
-    int64_t n = 0;
-    bool has_mask = false;
-    FilmDev fh{};
-    FilmDev* d_film = nullptr;
-    StepState* d_state = nullptr;
-    StepState* h_state = nullptr;  // pinned
+    int nf = 0;
+    std::vector<llg_grid> grids;
+    std::vector<llg_material> mats;
+    std::vector<FilmDev> fh;           // host mirror of the device descriptors
+    FilmDev* d_films = nullptr;
+    StepState* d_states = nullptr;
+    StepState* h_states = nullptr;     // pinned
+    RelaxStateDev* d_relax = nullptr;
+    RelaxStateDev* h_relax = nullptr;  // pinned
+    FilmCtl* d_ctl = nullptr;
+    FilmCtl* h_ctl = nullptr;          // pinned
     WorkItem* d_row_items = nullptr;
     WorkItem* d_col_items = nullptr;
     LaunchGeom geom{};
-    double* d_stage = nullptr;
-    double* d_k64 = nullptr;
+    double* d_stage = nullptr;         // AoS FP64 staging (largest film)
+    int64_t max_cells = 0;
+    bool any_demag = false;
+    std::vector<double*> d_k64;        // FP64 kernel planes per film (nullptr without demag)
     std::vector<void*> allocs;
-    std::vector<double> k64_host;
-    // host-side FSAL bookkeeping: the FSAL torque belongs to the last kind/mask/b_ext stepped
+    // host-side FSAL bookkeeping: the FSAL torque belongs to the last kind / mask / b_ext stepped
     int fsal_kind = 0;
     int fsal_mask = -1;
-    double fsal_bext[3] = {0, 0, 0};
-    bool last_b_eff_valid = false;  // relax: torque stats of the resident state are current
+    std::vector<double> fsal_bext;
     std::map<long long, cudaGraphExec_t> graphs;
     std::map<long long, cudaGraph_t> graph_defs;
     std::map<long long, long long> graph_kernels;  // kernel nodes per graph
-    long long launches = 0;                         // kernels issued on the stream so far
+    long long launches = 0;                         // kernels issued so far
+    bool l2_window = false;
+    cudaStreamAttrValue l2_attr{};
+    RelaxSettingsDev relax_graph_settings{};
 
-    int eval(const EvalSpec& e) {
-        CUDA_TRY(launch_eval<R>(e, geom, stream));
-        launches += (e.demag && geom.any_demag) ? 3 : 2;
-        return LLG_OK;
-    }
+    int nfilms() const override { return nf; }
+    int64_t cells(int f) const override { return grids[f].nx * grids[f].ny; }
 
     ~Engine() override {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
         for (auto& kv : graph_defs) cudaGraphDestroy(kv.second);
         for (void* p : allocs) cudaFree(p);
-        if (h_state) cudaFreeHost(h_state);
+        if (h_states) cudaFreeHost(h_states);
+        if (h_relax) cudaFreeHost(h_relax);
+        if (h_ctl) cudaFreeHost(h_ctl);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 
@@ -290,169 +311,209 @@ struct Engine final : EngineBase {
         return LLG_OK;
     }
 
-    int init(int dev, const llg_grid* g, const llg_material* m, const uint8_t* mask) {
+    int eval(const EvalSpec& e) {
+        CUDA_TRY(launch_eval<R>(e, geom, stream));
+        launches += (e.demag && geom.any_demag) ? 3 : 2;
+        return LLG_OK;
+    }
+
+    int init(int dev, int n_films, const llg_grid* g, const llg_material* m, const uint8_t* const* masks) {
         device = dev;
-        grid = *g;
-        mat = *m;
-        n = g->nx * g->ny;
-        const int nx = (int)g->nx, ny = (int)g->ny;
+        nf = n_films;
+        grids.assign(g, g + nf);
+        mats.assign(m, m + nf);
+        fh.assign(nf, FilmDev{});
+        d_k64.assign(nf, nullptr);
+        fsal_bext.assign(3 * (size_t)nf, 0.0);
         CUDA_TRY(cudaSetDevice(dev));
         CUDA_TRY(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
         stream = own_stream;
-        CUDA_TRY(cudaMallocHost(&h_state, sizeof(StepState)));
-        const bool demag = mat.demag != 0;
-        // register-FFT kernels for power-of-two sizes, generic kernels otherwise
-        const FastCfg fc = fast_config<R>(nx, ny);
-        const bool fast = fc.ok && !force_generic();
+        CUDA_TRY(cudaMallocHost(&h_states, sizeof(StepState) * nf));
+        CUDA_TRY(cudaMallocHost(&h_relax, sizeof(RelaxStateDev) * nf));
+        CUDA_TRY(cudaMallocHost(&h_ctl, sizeof(FilmCtl) * nf));
+        // kernel choice: register-FFT kernels when every film shares one power-of-two shape
+        bool same_shape = true;
+        for (int f = 1; f < nf; ++f) same_shape &= g[f].nx == g[0].nx && g[f].ny == g[0].ny;
+        for (int f = 0; f < nf; ++f) any_demag |= m[f].demag != 0;
+        const int nx0 = (int)g[0].nx, ny0 = (int)g[0].ny;
+        const FastCfg fc = fast_config<R>(nx0, ny0);
+        const bool fast = same_shape && fc.ok && !force_generic();
         const int T = fast ? fc.T : 2;
         const int NC = fast ? fc.NC : 1;
         const int G = T + (T + 1) / 2;
-        size_t smem_row = demag ? 4 * (size_t)G * nx * sizeof(cx<R>) : 0;
-        size_t smem_col = demag ? 12 * (size_t)ny * sizeof(cx<R>) : 0;
+        size_t smem_row = 0, smem_col = 0;
+        for (int f = 0; f < nf; ++f) {
+            if (!m[f].demag) continue;
+            smem_row = std::max(smem_row, 4 * (size_t)G * g[f].nx * sizeof(cx<R>));
+            smem_col = std::max(smem_col, 12 * (size_t)g[f].ny * sizeof(cx<R>));
+        }
         const size_t smem_max = 227 * 1024;
         if (!fast && (smem_row > smem_max || smem_col > smem_max))
-            return set_error(LLG_ERR_INVALID, "grid %dx%d exceeds the in-shared-memory FFT limit for this precision",
-                             nx, ny);
+            return set_error(LLG_ERR_INVALID, "a film exceeds the in-shared-memory FFT limit for this precision");
         int rc;
-        const size_t plane = sizeof(R) * 3 * (size_t)n;
-        FilmDev& F = fh;
-        std::memset(&F, 0, sizeof(F));
-        F.nx = nx;
-        F.ny = ny;
-        F.rows_per_block = T;
-        F.nblk = (ny + T - 1) / T;
-        F.dx = g->dx;
-        F.dy = g->dy;
-        F.dz = g->dz;
-        F.ms = m->ms;
-        F.a_ex = m->a_ex;
-        F.k_u = m->k_u;
-        F.dmi = m->has_dmi ? m->dmi : 0.0;
-        F.exch = (m->a_ex != 0.0 && m->ms != 0.0) ? 2.0 * m->a_ex / m->ms : 0.0;
-        F.has_eta = (m->has_dmi && m->dmi != 0.0) ? 1 : 0;
-        F.eta = (F.has_eta && m->a_ex != 0.0) ? m->dmi / (2.0 * m->a_ex) : 0.0;
-        F.dmi_avail = (m->has_dmi && m->dmi != 0.0 && m->ms != 0.0 && m->a_ex != 0.0) ? 1 : 0;
-        F.dmi_pref = F.dmi_avail ? 2.0 * m->dmi / m->ms : 0.0;
-        F.anis = (m->k_u != 0.0 && m->ms != 0.0) ? 2.0 * m->k_u / m->ms : 0.0;
-        for (int c = 0; c < 3; ++c) F.u[c] = m->easy_axis[c];
-        F.demag_mat = demag ? 1 : 0;
-        F.plan_row = make_plan(nx);
-        F.plan_col = make_plan(ny);
-        for (int b = 0; b < 2; ++b) {
-            if ((rc = dalloc(&F.m[b], plane))) return rc;
-            if ((rc = dalloc(&F.ms_buf[b], plane))) return rc;
-        }
-        for (int q = 1; q <= 7; ++q)
-            if ((rc = dalloc(&F.k[q], plane))) return rc;
-        for (void* p : {F.m[0], F.m[1], F.ms_buf[0], F.ms_buf[1]}) CUDA_TRY(cudaMemsetAsync(p, 0, plane, stream));
-        for (int q = 1; q <= 7; ++q) CUDA_TRY(cudaMemsetAsync(F.k[q], 0, plane, stream));
-        if ((rc = dalloc(&F.red_part, sizeof(double) * RED_NSLOT * (size_t)F.nblk))) return rc;
-        if ((rc = dalloc(&d_state, sizeof(StepState)))) return rc;
-        CUDA_TRY(cudaMemsetAsync(d_state, 0, sizeof(StepState), stream));
-        F.st = d_state;
-        if (mask) {
-            has_mask = true;
-            uint8_t* dm = nullptr;
-            if ((rc = dalloc(&dm, (size_t)n))) return rc;
-            std::vector<uint8_t> norm((size_t)n);
-            for (int64_t i = 0; i < n; ++i) norm[i] = mask[i] ? 1 : 0;
-            CUDA_TRY(cudaMemcpyAsync(dm, norm.data(), (size_t)n, cudaMemcpyHostToDevice, stream));
-            CUDA_TRY(cudaStreamSynchronize(stream));
-            F.mask = dm;
-            F.has_mask = 1;
-        }
-        if (demag) {
-            void* tw_row;
-            void* tw_col;
-            if ((rc = dalloc(&tw_row, sizeof(cx<R>) * 2 * (size_t)nx))) return rc;
-            if ((rc = dalloc(&tw_col, sizeof(cx<R>) * 2 * (size_t)ny))) return rc;
-            CUDA_TRY(launch_twiddles(tw_row, 2 * nx, sizeof(R) == 8, stream));
-            CUDA_TRY(launch_twiddles(tw_col, 2 * ny, sizeof(R) == 8, stream));
-            F.tw_row = tw_row;
-            F.tw_col = tw_col;
-            if (fast) {
-                void* twp_row;
-                void* twp_col;
-                if ((rc = dalloc(&twp_row, sizeof(cx<R>) * (size_t)std::max(fc.twp_row_size, 1)))) return rc;
-                if ((rc = dalloc(&twp_col, sizeof(cx<R>) * (size_t)std::max(fc.twp_col_size, 1)))) return rc;
-                CUDA_TRY(build_pass_tables<R>(twp_row, nx, twp_col, ny, stream));
-                F.twp_row = twp_row;
-                F.twp_col = twp_col;
+        if ((rc = dalloc(&d_states, sizeof(StepState) * nf))) return rc;
+        CUDA_TRY(cudaMemsetAsync(d_states, 0, sizeof(StepState) * nf, stream));
+        if ((rc = dalloc(&d_relax, sizeof(RelaxStateDev) * nf))) return rc;
+        if ((rc = dalloc(&d_ctl, sizeof(FilmCtl) * nf))) return rc;
+        std::vector<WorkItem> rows, cols;
+        for (int f = 0; f < nf; ++f) {
+            const int nx = (int)g[f].nx, ny = (int)g[f].ny;
+            const int64_t n = (int64_t)nx * ny;
+            max_cells = std::max(max_cells, n);
+            const size_t plane = sizeof(R) * 3 * (size_t)n;
+            FilmDev& F = fh[f];
+            F.nx = nx;
+            F.ny = ny;
+            F.rows_per_block = T;
+            F.nblk = (ny + T - 1) / T;
+            F.dx = g[f].dx;
+            F.dy = g[f].dy;
+            F.dz = g[f].dz;
+            F.ms = m[f].ms;
+            F.a_ex = m[f].a_ex;
+            F.k_u = m[f].k_u;
+            F.dmi = m[f].has_dmi ? m[f].dmi : 0.0;
+            F.exch = (m[f].a_ex != 0.0 && m[f].ms != 0.0) ? 2.0 * m[f].a_ex / m[f].ms : 0.0;
+            F.has_eta = (m[f].has_dmi && m[f].dmi != 0.0) ? 1 : 0;
+            F.eta = (F.has_eta && m[f].a_ex != 0.0) ? m[f].dmi / (2.0 * m[f].a_ex) : 0.0;
+            F.dmi_avail = (m[f].has_dmi && m[f].dmi != 0.0 && m[f].ms != 0.0 && m[f].a_ex != 0.0) ? 1 : 0;
+            F.dmi_pref = F.dmi_avail ? 2.0 * m[f].dmi / m[f].ms : 0.0;
+            F.anis = (m[f].k_u != 0.0 && m[f].ms != 0.0) ? 2.0 * m[f].k_u / m[f].ms : 0.0;
+            for (int c = 0; c < 3; ++c) F.u[c] = m[f].easy_axis[c];
+            F.demag_mat = m[f].demag ? 1 : 0;
+            F.plan_row = make_plan(nx);
+            F.plan_col = make_plan(ny);
+            for (int b = 0; b < 2; ++b) {
+                if ((rc = dalloc(&F.m[b], plane))) return rc;
+                if ((rc = dalloc(&F.ms_buf[b], plane))) return rc;
+                CUDA_TRY(cudaMemsetAsync(F.m[b], 0, plane, stream));
+                CUDA_TRY(cudaMemsetAsync(F.ms_buf[b], 0, plane, stream));
             }
-            if ((rc = dalloc(&F.X, sizeof(cx<R>) * 3 * (size_t)(nx + 1) * ny))) return rc;
-            void* kh;
-            if ((rc = dalloc(&kh, sizeof(r4<R>) * (size_t)(nx + 1) * (ny + 1)))) return rc;
-            F.Khat = kh;
-            if ((rc = dalloc(&d_k64, sizeof(double) * 4 * (size_t)(nx + 1) * (ny + 1)))) return rc;
-            CUDA_TRY(build_demag_kernel(nx, ny, g->dx, g->dy, g->dz, sizeof(R) == 8, kh, d_k64, stream));
-            if (fast) {
-                void* kp;
-                if ((rc = dalloc(&kp, sizeof(r4<R>) * (size_t)(nx + 1) * 2 * ny))) return rc;
-                CUDA_TRY(build_kernel_parity(nx, ny, sizeof(R) == 8, kh, kp, stream));
-                F.Kpar = kp;
+            for (int q = 1; q <= 7; ++q) {
+                if ((rc = dalloc(&F.k[q], plane))) return rc;
+                CUDA_TRY(cudaMemsetAsync(F.k[q], 0, plane, stream));
             }
+            if ((rc = dalloc(&F.red_part, sizeof(double) * RED_NSLOT * (size_t)F.nblk))) return rc;
+            F.st = d_states + f;
+            if (masks && masks[f]) {
+                uint8_t* dm = nullptr;
+                if ((rc = dalloc(&dm, (size_t)n))) return rc;
+                std::vector<uint8_t> norm((size_t)n);
+                for (int64_t i = 0; i < n; ++i) norm[i] = masks[f][i] ? 1 : 0;
+                CUDA_TRY(cudaMemcpyAsync(dm, norm.data(), (size_t)n, cudaMemcpyHostToDevice, stream));
+                CUDA_TRY(cudaStreamSynchronize(stream));
+                F.mask = dm;
+                F.has_mask = 1;
+            }
+            if (m[f].demag) {
+                void* tw_row;
+                void* tw_col;
+                if ((rc = dalloc(&tw_row, sizeof(cx<R>) * 2 * (size_t)nx))) return rc;
+                if ((rc = dalloc(&tw_col, sizeof(cx<R>) * 2 * (size_t)ny))) return rc;
+                CUDA_TRY(launch_twiddles(tw_row, 2 * nx, sizeof(R) == 8, stream));
+                CUDA_TRY(launch_twiddles(tw_col, 2 * ny, sizeof(R) == 8, stream));
+                F.tw_row = tw_row;
+                F.tw_col = tw_col;
+                if (fast) {
+                    void* twp_row;
+                    void* twp_col;
+                    if ((rc = dalloc(&twp_row, sizeof(cx<R>) * (size_t)std::max(fc.twp_row_size, 1)))) return rc;
+                    if ((rc = dalloc(&twp_col, sizeof(cx<R>) * (size_t)std::max(fc.twp_col_size, 1)))) return rc;
+                    CUDA_TRY(build_pass_tables<R>(twp_row, nx, twp_col, ny, stream));
+                    F.twp_row = twp_row;
+                    F.twp_col = twp_col;
+                }
+                if ((rc = dalloc(&F.X, sizeof(cx<R>) * 3 * (size_t)(nx + 1) * ny))) return rc;
+                // films sharing a grid share the kernel planes (get_demag_operator, demag_fft_uniform.rs:86)
+                int same = -1;
+                for (int e = 0; e < f && same < 0; ++e)
+                    if (mats[e].demag && grids[e].nx == nx && grids[e].ny == ny && grids[e].dx == g[f].dx &&
+                        grids[e].dy == g[f].dy && grids[e].dz == g[f].dz)
+                        same = e;
+                if (same >= 0) {
+                    F.Khat = fh[same].Khat;
+                    F.Kpar = fh[same].Kpar;
+                    d_k64[f] = d_k64[same];
+                } else {
+                    void* kh;
+                    if ((rc = dalloc(&kh, sizeof(r4<R>) * (size_t)(nx + 1) * (ny + 1)))) return rc;
+                    F.Khat = kh;
+                    if ((rc = dalloc(&d_k64[f], sizeof(double) * 4 * (size_t)(nx + 1) * (ny + 1)))) return rc;
+                    CUDA_TRY(build_demag_kernel(nx, ny, g[f].dx, g[f].dy, g[f].dz, sizeof(R) == 8, kh, d_k64[f],
+                                                stream));
+                    if (fast) {
+                        void* kp;
+                        if ((rc = dalloc(&kp, sizeof(r4<R>) * (size_t)(nx + 1) * 2 * ny))) return rc;
+                        CUDA_TRY(build_kernel_parity(nx, ny, sizeof(R) == 8, kh, kp, stream));
+                        F.Kpar = kp;
+                    }
+                }
+            }
+            for (int b = 0; b < F.nblk; ++b) rows.push_back(WorkItem{f, b});
+            const int ncb = (nx + 1 + NC - 1) / NC;
+            if (m[f].demag)
+                for (int b = 0; b < ncb; ++b) cols.push_back(WorkItem{f, b});
         }
-        if ((rc = dalloc(&d_film, sizeof(FilmDev)))) return rc;
-        CUDA_TRY(cudaMemcpyAsync(d_film, &F, sizeof(FilmDev), cudaMemcpyHostToDevice, stream));
-        const int ncol_blk = (nx + 1 + NC - 1) / NC;
-        std::vector<WorkItem> rows(F.nblk), cols(ncol_blk);
-        for (int b = 0; b < F.nblk; ++b) rows[b] = WorkItem{0, b};
-        for (int b = 0; b < ncol_blk; ++b) cols[b] = WorkItem{0, b};
-        if ((rc = dalloc(&d_row_items, sizeof(WorkItem) * rows.size()))) return rc;
-        if ((rc = dalloc(&d_col_items, sizeof(WorkItem) * cols.size()))) return rc;
+        if ((rc = dalloc(&d_films, sizeof(FilmDev) * nf))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(d_films, fh.data(), sizeof(FilmDev) * nf, cudaMemcpyHostToDevice, stream));
+        if ((rc = dalloc(&d_row_items, sizeof(WorkItem) * std::max<size_t>(rows.size(), 1)))) return rc;
+        if ((rc = dalloc(&d_col_items, sizeof(WorkItem) * std::max<size_t>(cols.size(), 1)))) return rc;
         CUDA_TRY(cudaMemcpyAsync(d_row_items, rows.data(), sizeof(WorkItem) * rows.size(), cudaMemcpyHostToDevice,
                                  stream));
-        CUDA_TRY(cudaMemcpyAsync(d_col_items, cols.data(), sizeof(WorkItem) * cols.size(), cudaMemcpyHostToDevice,
-                                 stream));
-        geom.films = d_film;
+        if (!cols.empty())
+            CUDA_TRY(cudaMemcpyAsync(d_col_items, cols.data(), sizeof(WorkItem) * cols.size(), cudaMemcpyHostToDevice,
+                                     stream));
+        geom.films = d_films;
         geom.row_items = d_row_items;
-        geom.n_row_items = F.nblk;
+        geom.n_row_items = (int)rows.size();
         geom.col_items = d_col_items;
-        geom.n_col_items = ncol_blk;
+        geom.n_col_items = (int)cols.size();
         geom.smem_row = smem_row;
         geom.smem_col = smem_col;
-        geom.grid_row = F.nblk;
-        geom.grid_col = ncol_blk;
-        geom.any_demag = demag;
-        geom.fast_row = fast ? nx : 0;
-        geom.fast_col = fast ? ny : 0;
+        geom.any_demag = any_demag;
+        geom.fast_row = fast ? nx0 : 0;
+        geom.fast_col = fast ? ny0 : 0;
         geom.row_threads = fast ? fc.row_threads : 256;
         geom.col_threads = fast ? fc.col_threads : 256;
         CUDA_TRY(prepare_eval_kernels<R>(fast ? 0 : smem_row, fast ? 0 : smem_col));
-        if (fast) {
-            // persistent grids: one wave of resident blocks looping over the work
-            // items, so the twiddle tables are loaded once per block
+        {
+            // persistent grids: one wave of resident blocks looping over the work items
             int nsm = 148, rb = 1, cb = 1;
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            fast_occupancy<R>(nx, ny, &rb, &cb);
-            geom.grid_row = std::min(F.nblk, nsm * rb);
-            geom.grid_col = std::min(ncol_blk, nsm * cb);
+            if (fast) {
+                fast_occupancy<R>(nx0, ny0, &rb, &cb);
+            } else {
+                rb = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_row, 1))));
+                cb = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_col, 1))));
+            }
+            geom.grid_row = std::max(1, std::min(geom.n_row_items, nsm * rb));
+            geom.grid_col = std::max(1, std::min(std::max(geom.n_col_items, 1), nsm * cb));
         }
-        if (demag) set_l2_window();
+        if (any_demag && nf == 1) set_l2_window();
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
     }
 
     // Keep the spectrum scratch (written by the row pass, read by the column
     // pass, read again by the row-inverse pass) resident in L2 across the
-    // passes of an evaluation.  The persisting carve-out is a property of this
+    // passes of an evaluation.  The persisting carve-out belongs to this
     // process's context only.
     void set_l2_window() {
-        int dev = device;
         int max_persist = 0, max_window = 0;
-        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev);
-        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev);
-        if (max_persist <= 0 || max_window <= 0 || !fh.X) return;
-        const size_t xbytes = sizeof(cx<R>) * 3 * (size_t)(fh.nx + 1) * fh.ny;
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, device);
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, device);
+        if (max_persist <= 0 || max_window <= 0 || !fh[0].X) return;
+        const size_t xbytes = sizeof(cx<R>) * 3 * (size_t)(fh[0].nx + 1) * fh[0].ny;
         size_t want = std::min<size_t>(xbytes, (size_t)max_persist);
         if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
             cudaGetLastError();
             return;
         }
         cudaStreamAttrValue attr{};
-        attr.accessPolicyWindow.base_ptr = fh.X;
+        attr.accessPolicyWindow.base_ptr = fh[0].X;
         attr.accessPolicyWindow.num_bytes = std::min<size_t>(xbytes, (size_t)max_window);
-        attr.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)want / (double)attr.accessPolicyWindow.num_bytes);
+        attr.accessPolicyWindow.hitRatio =
+            (float)std::min(1.0, (double)want / (double)attr.accessPolicyWindow.num_bytes);
         attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
         attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
         l2_attr = attr;
@@ -460,11 +521,9 @@ struct Engine final : EngineBase {
         if (cudaStreamSetAttribute(own_stream, cudaStreamAttributeAccessPolicyWindow, &attr) != cudaSuccess)
             cudaGetLastError();
     }
-    bool l2_window = false;
-    cudaStreamAttrValue l2_attr{};
 
-    int upload_film() {
-        CUDA_TRY(cudaMemcpyAsync(d_film, &fh, sizeof(FilmDev), cudaMemcpyHostToDevice, stream));
+    int upload_films() {
+        CUDA_TRY(cudaMemcpyAsync(d_films, fh.data(), sizeof(FilmDev) * nf, cudaMemcpyHostToDevice, stream));
         return LLG_OK;
     }
 
@@ -481,62 +540,37 @@ struct Engine final : EngineBase {
     }
 
     int ensure_stage() {
-        if (!d_stage) return dalloc(&d_stage, sizeof(double) * 3 * (size_t)n);
+        if (!d_stage) return dalloc(&d_stage, sizeof(double) * 3 * (size_t)max_cells);
         return LLG_OK;
     }
 
-    int set_state(const double* m) override {
-        int rc;
-        if ((rc = ensure_stage())) return rc;
-        CUDA_TRY(cudaMemcpyAsync(d_stage, m, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, stream));
-        k_aos_to_soa<R><<<592, 256, 0, stream>>>(d_film, d_stage);
-        CUDA_TRY(cudaGetLastError());
-        invalidate_fsal_host();
-        Control c = idle_control();
-        c.invalidate_fsal = 1;
-        k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
-        CUDA_TRY(cudaGetLastError());
-        launches += 1;
+    int read_states() {
+        CUDA_TRY(cudaMemcpyAsync(h_states, d_states, sizeof(StepState) * nf, cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
-        return LLG_OK;
-    }
-
-    int get_state(double* m) override {
-        int rc;
-        if ((rc = ensure_stage())) return rc;
-        k_soa_to_aos<R><<<592, 256, 0, stream>>>(d_film, 0, d_stage);
-        CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaMemcpyAsync(m, d_stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaStreamSynchronize(stream));
-        return LLG_OK;
-    }
-
-    int read_state() {
-        CUDA_TRY(cudaMemcpyAsync(h_state, d_state, sizeof(StepState), cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaStreamSynchronize(stream));
-        return LLG_OK;
-    }
-
-    int mean_m(double* out3) override {
-        k_mean_m<R><<<fh.nblk, 256, 0, stream>>>(d_film);
-        CUDA_TRY(cudaGetLastError());
-        k_finalize<<<1, 32, 0, stream>>>(d_film, 1);
-        CUDA_TRY(cudaGetLastError());
-        int rc;
-        if ((rc = read_state())) return rc;
-        for (int c = 0; c < 3; ++c) out3[c] = h_state->red[RED_MX + c] / (double)n;
         return LLG_OK;
     }
 
     void invalidate_fsal_host() {
         fsal_kind = 0;
         fsal_mask = -1;
-        last_b_eff_valid = false;
+    }
+
+    // Per-film control: dt from params (or kept) and FSAL invalidation flags.
+    int set_control(const Control& c, const llg_params* p, const bool* invalidate, bool keep_dt) {
+        for (int f = 0; f < nf; ++f) {
+            h_ctl[f].dt = p ? p[f].dt : 0.0;
+            h_ctl[f].keep_dt = (keep_dt || !p) ? 1 : 0;
+            h_ctl[f].invalidate_fsal = invalidate ? (invalidate[f] ? 1 : 0) : 0;
+        }
+        CUDA_TRY(cudaMemcpyAsync(d_ctl, h_ctl, sizeof(FilmCtl) * nf, cudaMemcpyHostToDevice, stream));
+        k_set_control<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, c, d_ctl);
+        CUDA_TRY(cudaGetLastError());
+        launches += 1;
+        return LLG_OK;
     }
 
     Control idle_control() {
         Control c{};
-        c.dt = 0.0;
         c.t_end = INFINITY;
         c.max_err = 1.0;
         c.headroom = 1.0;
@@ -544,24 +578,61 @@ struct Engine final : EngineBase {
         c.dt_max = 1.0;
         c.target_acc = -1;
         c.attempts = -1;
-        c.invalidate_fsal = 0;
         c.reset_time = 0;
         return c;
     }
 
-    // Sets gamma/alpha/b_ext of the film; returns true when b_ext changed.
-    int apply_params(const llg_params* p, bool* changed_bext) {
-        bool ch = fh.gamma != p->gamma || fh.alpha != p->alpha;
-        bool chb = fh.bext[0] != p->b_ext[0] || fh.bext[1] != p->b_ext[1] || fh.bext[2] != p->b_ext[2];
-        if (ch || chb) {
-            fh.gamma = p->gamma;
-            fh.alpha = p->alpha;
-            for (int c = 0; c < 3; ++c) fh.bext[c] = p->b_ext[c];
-            int rc = upload_film();
-            if (rc) return rc;
-        }
-        if (changed_bext) *changed_bext = chb;
+    int set_state(int f, const double* m) override {
+        int rc;
+        if ((rc = ensure_stage())) return rc;
+        CUDA_TRY(cudaMemcpyAsync(d_stage, m, sizeof(double) * 3 * (size_t)cells(f), cudaMemcpyHostToDevice, stream));
+        k_aos_to_soa<R><<<592, 256, 0, stream>>>(d_films, f, d_stage);
+        CUDA_TRY(cudaGetLastError());
+        invalidate_fsal_host();
+        std::unique_ptr<bool[]> iv(new bool[nf]);
+        for (int e = 0; e < nf; ++e) iv[e] = e == f;
+        if ((rc = set_control(idle_control(), nullptr, iv.get(), true))) return rc;
+        CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
+    }
+
+    int get_state(int f, double* m) override {
+        int rc;
+        if ((rc = ensure_stage())) return rc;
+        k_soa_to_aos<R><<<592, 256, 0, stream>>>(d_films, f, 0, d_stage);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(m, d_stage, sizeof(double) * 3 * (size_t)cells(f), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return LLG_OK;
+    }
+
+    int mean_m(double* out3n) override {
+        k_mean_m<R><<<std::min(geom.n_row_items, 148 * 8), 256, 0, stream>>>(d_films, d_row_items, geom.n_row_items);
+        CUDA_TRY(cudaGetLastError());
+        k_finalize<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, 0);
+        CUDA_TRY(cudaGetLastError());
+        int rc;
+        if ((rc = read_states())) return rc;
+        for (int f = 0; f < nf; ++f)
+            for (int c = 0; c < 3; ++c) out3n[3 * f + c] = h_states[f].red[RED_MX + c] / (double)cells(f);
+        return LLG_OK;
+    }
+
+    // Sets gamma / alpha / b_ext of every film.
+    int apply_params(const llg_params* p) {
+        bool any = false;
+        for (int f = 0; f < nf; ++f) {
+            FilmDev& F = fh[f];
+            bool ch = F.gamma != p[f].gamma || F.alpha != p[f].alpha || F.bext[0] != p[f].b_ext[0] ||
+                      F.bext[1] != p[f].b_ext[1] || F.bext[2] != p[f].b_ext[2];
+            if (ch) {
+                F.gamma = p[f].gamma;
+                F.alpha = p[f].alpha;
+                for (int c = 0; c < 3; ++c) F.bext[c] = p[f].b_ext[c];
+                any = true;
+            }
+        }
+        return any ? upload_films() : LLG_OK;
     }
 
     EvalSpec base_spec(int fmask) {
@@ -585,31 +656,40 @@ struct Engine final : EngineBase {
         for (double a : as) s.a[q++] = a;
     }
 
-    int launch_attempt(int kind, int fmask) {
+    int finalize(int req) {
+        k_finalize<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, req);
+        CUDA_TRY(cudaGetLastError());
+        launches += 1;
+        return LLG_OK;
+    }
+
+    // One integrator attempt; req gates every kernel on StepState::req (relax).
+    int launch_attempt(int kind, int fmask, int req) {
+        int rc;
         EvalSpec e = base_spec(fmask);
-        const int rhs = kind == KIND_RK45 ? RHS_LLG : RHS_RELAX;
-        e.rhs = rhs;
+        e.req = req;
+        e.rhs = kind == KIND_RK45 ? RHS_LLG : RHS_RELAX;
         e.k_out = KB_K1;
         e.skip_if_fsal = 1;
-        { int _rc = eval(e); if (_rc) return _rc; }
+        if ((rc = eval(e))) return rc;
         e.skip_if_fsal = 0;
         if (kind == KIND_RK45) {
             using namespace dp5;
             combo(e, MB_S0, {KB_K1}, {A21});
             e.k_out = KB_K2;
-            { int _rc = eval(e); if (_rc) return _rc; }
+            if ((rc = eval(e))) return rc;
             combo(e, MB_S1, {KB_K1, KB_K2}, {A31, A32});
             e.k_out = KB_K3;
-            { int _rc = eval(e); if (_rc) return _rc; }
+            if ((rc = eval(e))) return rc;
             combo(e, MB_S0, {KB_K1, KB_K2, KB_K3}, {A41, A42, A43});
             e.k_out = KB_K4;
-            { int _rc = eval(e); if (_rc) return _rc; }
+            if ((rc = eval(e))) return rc;
             combo(e, MB_S1, {KB_K1, KB_K2, KB_K3, KB_K4}, {A51, A52, A53, A54});
             e.k_out = KB_K5;
-            { int _rc = eval(e); if (_rc) return _rc; }
+            if ((rc = eval(e))) return rc;
             combo(e, MB_S0, {KB_K1, KB_K2, KB_K3, KB_K4, KB_K5}, {A61, A62, A63, A64, A65});
             e.k_out = KB_K6;
-            { int _rc = eval(e); if (_rc) return _rc; }
+            if ((rc = eval(e))) return rc;
             combo(e, MB_M7, {KB_K1, KB_K3, KB_K4, KB_K5, KB_K6}, {B1, B3, B4, B5, B6});
             e.k_out = KB_K7;
             e.err = ERR_RK45;
@@ -617,18 +697,18 @@ struct Engine final : EngineBase {
             const double wh[8] = {0, BH1, 0, BH3, BH4, BH5, BH6, BH7};
             std::memcpy(e.wb, wb, sizeof(wb));
             std::memcpy(e.wh, wh, sizeof(wh));
-            { int _rc = eval(e); if (_rc) return _rc; }
-            k_controller<<<1, 32, 0, stream>>>(d_film, 1, 5);
+            if ((rc = eval(e))) return rc;
+            k_controller<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, 5, req);
             CUDA_TRY(cudaGetLastError());
             launches += 1;
         } else {
             using namespace bs3;
             combo(e, MB_S0, {KB_K1}, {A21});
             e.k_out = KB_K2;
-            { int _rc = eval(e); if (_rc) return _rc; }
+            if ((rc = eval(e))) return rc;
             combo(e, MB_S1, {KB_K2}, {A32});
             e.k_out = KB_K3;
-            { int _rc = eval(e); if (_rc) return _rc; }
+            if ((rc = eval(e))) return rc;
             combo(e, MB_M7, {KB_K1, KB_K2, KB_K3}, {B1, B2, B3});
             e.k_out = KB_K7;
             e.err = ERR_RK23;
@@ -637,13 +717,35 @@ struct Engine final : EngineBase {
             const double wh[8] = {0, BH1, BH2, BH3, BH4, 0, 0, 0};
             std::memcpy(e.wb, wb, sizeof(wb));
             std::memcpy(e.wh, wh, sizeof(wh));
-            { int _rc = eval(e); if (_rc) return _rc; }
-            k_controller<<<1, 32, 0, stream>>>(d_film, 1, 3);
+            if ((rc = eval(e))) return rc;
+            k_controller<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, 3, req);
             CUDA_TRY(cudaGetLastError());
-            k_finalize<<<1, 32, 0, stream>>>(d_film, 1);
-            CUDA_TRY(cudaGetLastError());
-            launches += 2;
+            launches += 1;
+            if ((rc = finalize(req))) return rc;
         }
+        return LLG_OK;
+    }
+
+    // One relax iteration: the request-gated energy, torque and RK23 step, then the controller.
+    int launch_relax_iteration(int fmask, const RelaxSettingsDev& S) {
+        int rc;
+        EvalSpec en = base_spec(LLG_FIELD_FULL);
+        en.req = REQ_ENERGY;
+        en.rhs = RHS_ENERGY;
+        en.reduce = 1;
+        en.demag = 1;  // the energy includes demag iff Material::demag (energy.rs:117-121)
+        if ((rc = eval(en))) return rc;
+        if ((rc = finalize(REQ_ENERGY))) return rc;
+        EvalSpec tq = base_spec(fmask);
+        tq.req = REQ_TORQUE;
+        tq.rhs = RHS_TORQUE;
+        tq.reduce = 1;
+        if ((rc = eval(tq))) return rc;
+        if ((rc = finalize(REQ_TORQUE))) return rc;
+        if ((rc = launch_attempt(KIND_RK23, fmask, REQ_STEP))) return rc;
+        k_relax_control<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, d_relax, nf, S);
+        CUDA_TRY(cudaGetLastError());
+        launches += 1;
         return LLG_OK;
     }
 
@@ -653,13 +755,13 @@ struct Engine final : EngineBase {
         return LLG_OK;
     }
 
-    // Graph of `reps` back-to-back attempts.
     static long long graph_key(int kind, int fmask, int reps) {
         return ((long long)kind << 40) | ((long long)fmask << 32) | (long long)reps;
     }
 
-    int attempt_graph(int kind, int fmask, int reps, cudaGraphExec_t* out) {
-        long long key = graph_key(kind, fmask, reps);
+    // Graph of `reps` back-to-back attempts (or relax iterations).
+    template <typename Body>
+    int get_graph(long long key, int reps, Body body, cudaGraphExec_t* out) {
         auto it = graphs.find(key);
         if (it != graphs.end()) {
             *out = it->second;
@@ -672,7 +774,7 @@ struct Engine final : EngineBase {
         stream = cap;
         int rc = LLG_OK;
         const long long before = launches;
-        for (int r = 0; r < reps && rc == LLG_OK; ++r) rc = launch_attempt(kind, fmask);
+        for (int r = 0; r < reps && rc == LLG_OK; ++r) rc = body();
         graph_kernels[key] = launches - before;
         launches = before;
         stream = saved;
@@ -691,53 +793,57 @@ struct Engine final : EngineBase {
         return LLG_OK;
     }
 
-    int prepare_step(int kind, const llg_params* p, int fmask, Control* c) {
-        bool chb = false;
-        int rc = apply_params(p, &chb);
-        if (rc) return rc;
-        bool same = fsal_kind == kind && fsal_mask == fmask && fsal_bext[0] == p->b_ext[0] &&
-                    fsal_bext[1] == p->b_ext[1] && fsal_bext[2] == p->b_ext[2];
-        c->invalidate_fsal = same ? 0 : 1;
-        return LLG_OK;
+    int attempt_graph(int kind, int fmask, int reps, cudaGraphExec_t* out) {
+        return get_graph(graph_key(kind, fmask, reps), reps, [&]() { return launch_attempt(kind, fmask, 0); }, out);
+    }
+
+    // FSAL validity across calls (llg.rs:854-867, 317-330): same kind, mask and b_ext.
+    void fsal_flags(int kind, const llg_params* p, int fmask, bool* inval) {
+        for (int f = 0; f < nf; ++f) {
+            bool same = fsal_kind == kind && fsal_mask == fmask && fsal_bext[3 * f] == p[f].b_ext[0] &&
+                        fsal_bext[3 * f + 1] == p[f].b_ext[1] && fsal_bext[3 * f + 2] == p[f].b_ext[2];
+            inval[f] = !same;
+        }
     }
 
     void note_fsal(int kind, int fmask, const llg_params* p) {
         fsal_kind = kind;
         fsal_mask = fmask;
-        for (int c = 0; c < 3; ++c) fsal_bext[c] = p->b_ext[c];
+        for (int f = 0; f < nf; ++f)
+            for (int c = 0; c < 3; ++c) fsal_bext[3 * f + c] = p[f].b_ext[c];
     }
 
     int step(int kind, llg_params* p, int fmask, double max_err, double headroom, double dt_min, double dt_max,
              double* eps, int32_t* acc, double* dtu) override {
         if (fmask < 0 || fmask > 2) return set_error(LLG_ERR_INVALID, "bad field mask %d", fmask);
+        int rc;
+        if ((rc = apply_params(p))) return rc;
         Control c = idle_control();
-        c.dt = p->dt;
         c.max_err = max_err;
         c.headroom = headroom;
         c.dt_min = dt_min;
         c.dt_max = dt_max;
         c.attempts = 1;
-        int rc = prepare_step(kind, p, fmask, &c);
-        if (rc) return rc;
-        k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
-        CUDA_TRY(cudaGetLastError());
-        launches += 1;
+        std::unique_ptr<bool[]> inv(new bool[nf]);
+        fsal_flags(kind, p, fmask, inv.get());
+        if ((rc = set_control(c, p, inv.get(), false))) return rc;
         cudaGraphExec_t ge = nullptr;
         if ((rc = attempt_graph(kind, fmask, 1, &ge))) return rc;
         if ((rc = graph_launch(graph_key(kind, fmask, 1), ge))) return rc;
-        if ((rc = read_state())) return rc;
-        const StepState& s = *h_state;
-        if (s.err_code) {
-            invalidate_fsal_host();
-            return set_error(s.err_code, "non-finite error norm (NaN/Inf in the state or field)");
+        if ((rc = read_states())) return rc;
+        for (int f = 0; f < nf; ++f) {
+            const StepState& s = h_states[f];
+            if (s.err_code) {
+                invalidate_fsal_host();
+                return set_error(s.err_code, "film %d: non-finite error norm (NaN/Inf in the state or field)", f);
+            }
+            eps[f] = s.eps;
+            acc[f] = s.accepted;
+            dtu[f] = s.dt_used;
+            p[f].dt = s.dt;
         }
-        *eps = s.eps;
-        *acc = s.accepted;
-        *dtu = s.dt_used;
-        p->dt = s.dt;
-        if (s.accepted) note_fsal(kind, fmask, p);
-        else invalidate_fsal_host();
-        last_b_eff_valid = kind == KIND_RK23 && s.accepted;
+        // per-film FSAL validity is tracked on the device; the host tracks kind / mask / b_ext
+        note_fsal(kind, fmask, p);
         return LLG_OK;
     }
 
@@ -746,10 +852,14 @@ struct Engine final : EngineBase {
             double* t_adv) override {
         if (fmask < 0 || fmask > 2) return set_error(LLG_ERR_INVALID, "bad field mask %d", fmask);
         int rc;
-        if ((rc = read_state())) return rc;
-        const long long acc0 = h_state->n_acc, rej0 = h_state->n_rej;
+        if ((rc = apply_params(p))) return rc;
+        if ((rc = read_states())) return rc;
+        std::vector<long long> acc0(nf), rej0(nf);
+        for (int f = 0; f < nf; ++f) {
+            acc0[f] = h_states[f].n_acc;
+            rej0[f] = h_states[f].n_rej;
+        }
         Control c = idle_control();
-        c.dt = p->dt;
         c.t_end = t_end;
         c.max_err = max_err;
         c.headroom = headroom;
@@ -758,87 +868,184 @@ struct Engine final : EngineBase {
         c.target_acc = n_acc;
         c.attempts = max_attempts > 0 ? max_attempts : -1;
         c.reset_time = 1;
-        if ((rc = prepare_step(kind, p, fmask, &c))) return rc;
-        k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
-        CUDA_TRY(cudaGetLastError());
-        launches += 1;
+        std::unique_ptr<bool[]> inv(new bool[nf]);
+        fsal_flags(kind, p, fmask, inv.get());
+        if ((rc = set_control(c, p, inv.get(), false))) return rc;
         const int reps = 8;
         cudaGraphExec_t ge = nullptr;
         if ((rc = attempt_graph(kind, fmask, reps, &ge))) return rc;
         long long launched = 0;
         const long long limit = max_attempts > 0 ? max_attempts : (1LL << 40);
         for (;;) {
-            // several graph launches between polls
             for (int q = 0; q < 4 && launched < limit; ++q) {
                 if ((rc = graph_launch(graph_key(kind, fmask, reps), ge))) return rc;
                 launched += reps;
             }
-            if ((rc = read_state())) return rc;
-            if (!h_state->active || launched >= limit) break;
+            if ((rc = read_states())) return rc;
+            bool any = false;
+            for (int f = 0; f < nf; ++f) any |= h_states[f].active != 0;
+            if (!any || launched >= limit) break;
         }
-        const StepState& s = *h_state;
-        *acc_out = s.n_acc - acc0;
-        *rej_out = s.n_rej - rej0;
-        *t_adv = s.t;
-        p->dt = s.dt;
-        if (s.err_code) {
-            invalidate_fsal_host();
-            return set_error(s.err_code, "non-finite error norm (NaN/Inf in the state or field)");
+        for (int f = 0; f < nf; ++f) {
+            const StepState& s = h_states[f];
+            acc_out[f] = s.n_acc - acc0[f];
+            rej_out[f] = s.n_rej - rej0[f];
+            t_adv[f] = s.t;
+            p[f].dt = s.dt;
+            if (s.err_code) {
+                invalidate_fsal_host();
+                return set_error(s.err_code, "film %d: non-finite error norm (NaN/Inf in the state or field)", f);
+            }
         }
-        if (s.fsal_valid) note_fsal(kind, fmask, p);
-        else invalidate_fsal_host();
-        last_b_eff_valid = false;
+        note_fsal(kind, fmask, p);
+        return LLG_OK;
+    }
+
+    // relax_with_report (relax.rs:334-768) for every film, on the device.
+    int relax(llg_params* p, int fmask, const llg_relax_settings* st, llg_relax_report* rep) override {
+        if (fmask < 0 || fmask > 2) return set_error(LLG_ERR_INVALID, "bad field mask %d", fmask);
+        int rc;
+        if ((rc = apply_params(p))) return rc;
+        RelaxSettingsDev S{};
+        S.max_err = st->max_err;
+        S.headroom = st->headroom;
+        S.dt_min = st->dt_min;
+        S.dt_max = st->dt_max;
+        S.rel_energy_tol = st->rel_energy_tol;
+        S.thr = st->torque_threshold;
+        S.plateau_rel = st->torque_plateau_rel;
+        S.plateau_abs = st->torque_plateau_abs;
+        S.tighten_factor = st->tighten_factor;
+        S.tighten_floor = st->tighten_floor;
+        S.gate = st->final_torque_gate;
+        S.gate_max = st->final_torque_gate_max;
+        S.energy_stride = st->energy_stride;
+        S.check_stride = st->torque_check_stride;
+        S.plateau_checks = st->torque_plateau_checks;
+        S.plateau_min_checks = st->torque_plateau_min_checks;
+        S.max_acc = st->max_accepted_steps;
+        S.gate_extra = st->gate_max_extra_accepted_steps;
+        S.gate_plateau_fails = st->gate_plateau_fails;
+        S.phase1 = st->phase1_enabled;
+        S.phase2 = st->phase2_enabled;
+        S.metric = st->torque_metric;
+        S.has_thr = st->has_torque_threshold;
+        S.has_gate = st->has_final_torque_gate;
+        S.has_gmax = st->has_final_torque_gate_max;
+        for (int f = 0; f < nf; ++f) {
+            std::memset(&h_relax[f], 0, sizeof(RelaxStateDev));
+            h_relax[f].pc = RP_START;
+            h_relax[f].last_stage = -1;
+            h_relax[f].max_err = st->max_err;
+            h_relax[f].n_cells = (double)cells(f);
+            p[f].dt = std::min(std::max(p[f].dt, st->dt_min), st->dt_max);  // relax.rs:373
+        }
+        CUDA_TRY(cudaMemcpyAsync(d_relax, h_relax, sizeof(RelaxStateDev) * nf, cudaMemcpyHostToDevice, stream));
+        Control c = idle_control();
+        c.max_err = st->max_err;
+        c.headroom = st->headroom;
+        c.dt_min = st->dt_min;
+        c.dt_max = st->dt_max;
+        std::unique_ptr<bool[]> inv(new bool[nf]);
+        for (int f = 0; f < nf; ++f) inv[f] = true;  // scratch.invalidate_last_b_eff() (relax.rs:374)
+        invalidate_fsal_host();
+        if ((rc = set_control(c, p, inv.get(), false))) return rc;
+        // issue the first requests
+        k_relax_control<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, d_relax, nf, S);
+        CUDA_TRY(cudaGetLastError());
+        launches += 1;
+        const int reps = 8;
+        const long long key = graph_key(KIND_RELAX, fmask, reps);
+        // the graph bakes the settings into the controller launches: rebuild when they differ
+        if (graphs.count(key) && std::memcmp(&relax_graph_settings, &S, sizeof(S)) != 0) {
+            cudaGraphExecDestroy(graphs[key]);
+            cudaGraphDestroy(graph_defs[key]);
+            graphs.erase(key);
+            graph_defs.erase(key);
+        }
+        relax_graph_settings = S;
+        cudaGraphExec_t ge = nullptr;
+        if ((rc = get_graph(key, reps, [&]() { return launch_relax_iteration(fmask, S); }, &ge))) return rc;
+        // Each iteration executes one request per film; accepted steps are capped by
+        // max_accepted_steps and every step size reaches dt_min within a bounded number
+        // of rejections, so this bound is only a safety net against a stuck film.
+        const long long max_iters = 16 * std::max<long long>(st->max_accepted_steps, 1) + 1000000;
+        long long iters = 0;
+        for (;;) {
+            for (int q = 0; q < 4; ++q)
+                if ((rc = graph_launch(key, ge))) return rc;
+            iters += 4 * reps;
+            if (iters > max_iters)
+                return set_error(LLG_ERR_TIMEOUT, "relax did not finish within %lld iterations", max_iters);
+            CUDA_TRY(cudaMemcpyAsync(h_relax, d_relax, sizeof(RelaxStateDev) * nf, cudaMemcpyDeviceToHost, stream));
+            if ((rc = read_states())) return rc;
+            bool all = true;
+            for (int f = 0; f < nf; ++f) all &= (h_relax[f].done != 0) || h_states[f].err_code != 0;
+            if (all) break;
+        }
+        for (int f = 0; f < nf; ++f) {
+            const RelaxStateDev& Q = h_relax[f];
+            const StepState& s = h_states[f];
+            if (s.err_code) return set_error(s.err_code, "film %d: non-finite error norm during relax", f);
+            rep[f].accepted_steps = Q.accepted;
+            rep[f].rejected_steps = Q.rejected;
+            rep[f].torque_checks = Q.checks;
+            rep[f].torque_field_rebuilds = Q.rebuilds;
+            rep[f].stop_reason = Q.stop_reason;
+            rep[f].last_stage_stop = Q.last_stage;
+            rep[f].has_final_torque = Q.has_ft;
+            rep[f].final_torque = Q.ft;
+            rep[f].has_final_torque_max = Q.has_ftm;
+            rep[f].final_torque_max = Q.ftm;
+            rep[f].final_max_err = Q.max_err;
+            rep[f].final_dt = s.dt;
+            p[f].dt = s.dt;
+        }
+        note_fsal(KIND_RK23, fmask, p);
         return LLG_OK;
     }
 
     int ensure_bout() {
-        if (!fh.bout) {
-            int rc = dalloc(&fh.bout, sizeof(R) * 3 * (size_t)n);
-            if (rc) return rc;
-            return upload_film();
+        bool any = false;
+        for (int f = 0; f < nf; ++f) {
+            if (!fh[f].bout) {
+                int rc = dalloc(&fh[f].bout, sizeof(R) * 3 * (size_t)cells(f));
+                if (rc) return rc;
+                any = true;
+            }
         }
-        return LLG_OK;
+        return any ? upload_films() : LLG_OK;
     }
 
-    // Runs one evaluation of the resident state with an idle controller.
+    // Runs one evaluation of the resident states with an idle controller (dt kept).
     int eval_resident(const EvalSpec& e) {
-        Control c = idle_control();
-        c.dt = 0.0;
-        // keep the device dt: read it back first so that set_control preserves it
         int rc;
-        if ((rc = read_state())) return rc;
-        c.dt = h_state->dt;
-        k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
-        CUDA_TRY(cudaGetLastError());
-        launches += 1;
-        { int _rc = eval(e); if (_rc) return _rc; }
-        if (e.reduce) {
-            k_finalize<<<1, 32, 0, stream>>>(d_film, 1);
-            CUDA_TRY(cudaGetLastError());
-        }
+        if ((rc = set_control(idle_control(), nullptr, nullptr, true))) return rc;
+        if ((rc = eval(e))) return rc;
+        if (e.reduce && (rc = finalize(0))) return rc;
         return LLG_OK;
     }
 
-    int build_h_eff(const llg_params* p, int fmask, double* b) override {
+    int build_h_eff(int f, const llg_params* p, int fmask, double* b) override {
         if (fmask < 0 || fmask > 2) return set_error(LLG_ERR_INVALID, "bad field mask %d", fmask);
         int rc;
-        if ((rc = apply_params(p, nullptr))) return rc;
+        if ((rc = apply_params(p))) return rc;
         if ((rc = ensure_bout())) return rc;
         if ((rc = ensure_stage())) return rc;
         EvalSpec e = base_spec(fmask);
         e.rhs = RHS_FIELD;
         if ((rc = eval_resident(e))) return rc;
-        k_soa_to_aos<R><<<592, 256, 0, stream>>>(d_film, 1, d_stage);
+        k_soa_to_aos<R><<<592, 256, 0, stream>>>(d_films, f, 1, d_stage);
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaMemcpyAsync(b, d_stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(b, d_stage, sizeof(double) * 3 * (size_t)cells(f), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
     }
 
-    int demag_field(double* b) override {
+    int demag_field(int f, double* b) override {
         int rc;
-        if (!mat.demag) {
-            std::memset(b, 0, sizeof(double) * 3 * (size_t)n);
+        if (!mats[f].demag) {
+            std::memset(b, 0, sizeof(double) * 3 * (size_t)cells(f));
             return LLG_OK;
         }
         if ((rc = ensure_bout())) return rc;
@@ -847,67 +1054,68 @@ struct Engine final : EngineBase {
         e.rhs = RHS_FIELD;
         e.local = 0;
         if ((rc = eval_resident(e))) return rc;
-        k_soa_to_aos<R><<<592, 256, 0, stream>>>(d_film, 1, d_stage);
+        k_soa_to_aos<R><<<592, 256, 0, stream>>>(d_films, f, 1, d_stage);
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaMemcpyAsync(b, d_stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(b, d_stage, sizeof(double) * 3 * (size_t)cells(f), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
     }
 
-    int energy(const double* bext, llg_energy_breakdown* out) override {
+    int energy(const double* bext3n, llg_energy_breakdown* out) override {
         // compute_energy_geom (energy.rs:80-285): demag enters iff Material::demag
-        llg_params p{};
-        p.gamma = fh.gamma;
-        p.alpha = fh.alpha;
-        for (int c = 0; c < 3; ++c) p.b_ext[c] = bext[c];
+        std::vector<llg_params> p(nf);
+        for (int f = 0; f < nf; ++f) {
+            p[f].gamma = fh[f].gamma;
+            p[f].alpha = fh[f].alpha;
+            for (int c = 0; c < 3; ++c) p[f].b_ext[c] = bext3n[3 * f + c];
+        }
         int rc;
-        if ((rc = apply_params(&p, nullptr))) return rc;
+        if ((rc = apply_params(p.data()))) return rc;
         EvalSpec e = base_spec(LLG_FIELD_FULL);
-        e.demag = mat.demag ? 1 : 0;
+        e.demag = 1;
         e.rhs = RHS_ENERGY;
         e.reduce = 1;
         if ((rc = eval_resident(e))) return rc;
-        if ((rc = read_state())) return rc;
-        out->exchange = h_state->red[RED_E_EX];
-        out->anisotropy = h_state->red[RED_E_AN];
-        out->zeeman = h_state->red[RED_E_ZEE];
-        out->dmi = h_state->red[RED_E_DMI];
-        out->demag = h_state->red[RED_E_DEMAG];
+        if ((rc = read_states())) return rc;
+        for (int f = 0; f < nf; ++f) {
+            out[f].exchange = h_states[f].red[RED_E_EX];
+            out[f].anisotropy = h_states[f].red[RED_E_AN];
+            out[f].zeeman = h_states[f].red[RED_E_ZEE];
+            out[f].dmi = h_states[f].red[RED_E_DMI];
+            out[f].demag = h_states[f].red[RED_E_DEMAG];
+        }
         return LLG_OK;
     }
 
-    double metric_from(const StepState& s, int metric) {
-        const double nf = (double)n;
+    static double torque_from_host(int metric, double tmax, double tsum, double tsum2, double n) {
         switch (metric) {
-            case LLG_TORQUE_MAX: return s.red[RED_TMAX];
-            case LLG_TORQUE_MEAN: return s.red[RED_TSUM] / std::max(nf, 1.0);
-            case LLG_TORQUE_RMS: return std::sqrt(s.red[RED_TSUM2] / std::max(nf, 1.0));
-            default: return s.red[RED_TSUM2] / std::max(nf, 1.0);
+            case LLG_TORQUE_MAX: return tmax;
+            case LLG_TORQUE_MEAN: return tsum / std::max(n, 1.0);
+            case LLG_TORQUE_RMS: return std::sqrt(tsum2 / std::max(n, 1.0));
+            default: return tsum2 / std::max(n, 1.0);
         }
     }
 
     int torque_metric(const llg_params* p, int fmask, int metric, double* out) override {
         int rc;
-        if ((rc = apply_params(p, nullptr))) return rc;
+        if ((rc = apply_params(p))) return rc;
         EvalSpec e = base_spec(fmask);
         e.rhs = RHS_TORQUE;
         e.reduce = 1;
         if ((rc = eval_resident(e))) return rc;
-        if ((rc = read_state())) return rc;
-        *out = metric_from(*h_state, metric);
+        if ((rc = read_states())) return rc;
+        for (int f = 0; f < nf; ++f)
+            out[f] = torque_from_host(metric, h_states[f].red[RED_TMAX], h_states[f].red[RED_TSUM],
+                                      h_states[f].red[RED_TSUM2], (double)cells(f));
         return LLG_OK;
     }
 
-    // Per-kernel CUDA-event timing of one representative RK45 stage evaluation
+    // Per-pass CUDA-event timing of one representative RK45 stage evaluation
     // (stage 4: three-term combination) repeated `reps` times on the stream.
     int profile_stage(const llg_params* p, int fmask, int reps, double* ms3) override {
         int rc;
-        if ((rc = apply_params(p, nullptr))) return rc;
-        Control c = idle_control();
-        if ((rc = read_state())) return rc;
-        c.dt = h_state->dt > 0 ? h_state->dt : p->dt;
-        k_set_control<<<1, 32, 0, stream>>>(d_film, 1, c);
-        CUDA_TRY(cudaGetLastError());
+        if ((rc = apply_params(p))) return rc;
+        if ((rc = set_control(idle_control(), nullptr, nullptr, true))) return rc;
         EvalSpec e = base_spec(fmask);
         e.rhs = RHS_LLG;
         combo(e, MB_S0, {KB_K1, KB_K2, KB_K3}, {dp5::A41, dp5::A42, dp5::A43});
@@ -917,11 +1125,11 @@ struct Engine final : EngineBase {
         double acc[3] = {0, 0, 0};
         for (int r = 0; r < reps; ++r) {
             CUDA_TRY(cudaEventRecord(ev[0], stream));
-            k_row_forward_launch(e);
+            CUDA_TRY(launch_one<R>(0, e, geom, stream));
             CUDA_TRY(cudaEventRecord(ev[1], stream));
-            if (e.demag && geom.any_demag) k_column_launch(e);
+            if (e.demag && geom.any_demag) CUDA_TRY(launch_one<R>(1, e, geom, stream));
             CUDA_TRY(cudaEventRecord(ev[2], stream));
-            k_row_inverse_launch(e);
+            CUDA_TRY(launch_one<R>(2, e, geom, stream));
             CUDA_TRY(cudaEventRecord(ev[3], stream));
             CUDA_TRY(cudaEventSynchronize(ev[3]));
             for (int q = 0; q < 3; ++q) {
@@ -934,206 +1142,15 @@ struct Engine final : EngineBase {
         for (int q = 0; q < 3; ++q) ms3[q] = acc[q] / reps;
         return LLG_OK;
     }
-    void k_row_forward_launch(const EvalSpec& e) { launch_one<R>(0, e, geom, stream); }
-    void k_column_launch(const EvalSpec& e) { launch_one<R>(1, e, geom, stream); }
-    void k_row_inverse_launch(const EvalSpec& e) { launch_one<R>(2, e, geom, stream); }
 
     long long launch_count() override { return launches; }
 
-    int kernel_kspace(double* out) override {
-        if (!mat.demag || !d_k64) return set_error(LLG_ERR_INVALID, "material has demag disabled");
-        size_t cnt = 4 * (size_t)(grid.nx + 1) * (grid.ny + 1);
-        CUDA_TRY(cudaMemcpyAsync(out, d_k64, sizeof(double) * cnt, cudaMemcpyDeviceToHost, stream));
+    int kernel_kspace(int f, double* out) override {
+        if (!mats[f].demag || !d_k64[f]) return set_error(LLG_ERR_INVALID, "material has demag disabled");
+        size_t cnt = 4 * (size_t)(grids[f].nx + 1) * (grids[f].ny + 1);
+        CUDA_TRY(cudaMemcpyAsync(out, d_k64[f], sizeof(double) * cnt, cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
-    }
-
-    // relax_with_report (relax.rs:334-768) driving the GPU RK23 attempts.
-    int relax(llg_params* p, int fmask, llg_relax_settings* st, llg_relax_report* rep) override {
-        const bool phase1 = st->phase1_enabled != 0, phase2 = st->phase2_enabled != 0;
-        const int64_t energy_stride = std::max<int64_t>(st->energy_stride, 1);
-        const int metric = st->torque_metric;
-        const bool has_thr = st->has_torque_threshold != 0;
-        const double thr = st->torque_threshold;
-        const int64_t check_stride = std::max<int64_t>(st->torque_check_stride, 1);
-        const double plateau_rel = st->torque_plateau_rel, plateau_abs = st->torque_plateau_abs;
-        const int64_t plateau_checks = st->torque_plateau_checks;
-        const int64_t plateau_min_checks = std::max<int64_t>(st->torque_plateau_min_checks, 1);
-        const int64_t max_acc = st->max_accepted_steps;
-        double max_err = st->max_err;
-        p->dt = std::min(std::max(p->dt, st->dt_min), st->dt_max);
-        invalidate_fsal_host();  // scratch.invalidate_last_b_eff()
-        int64_t accepted = 0, rejected = 0, checks = 0, rebuilds = 0;
-        int last_stage = -1;
-        bool has_ft = false, has_ftm = false;
-        double ft = 0.0, ftm = 0.0;
-        double torque_cache[RED_NSLOT];
-        int rc = LLG_OK;
-        auto finish = [&](int reason) {
-            st->max_err = max_err;
-            rep->accepted_steps = accepted;
-            rep->rejected_steps = rejected;
-            rep->torque_checks = checks;
-            rep->torque_field_rebuilds = rebuilds;
-            rep->stop_reason = reason;
-            rep->last_stage_stop = last_stage;
-            rep->has_final_torque = has_ft;
-            rep->final_torque = ft;
-            rep->has_final_torque_max = has_ftm;
-            rep->final_torque_max = ftm;
-            rep->final_max_err = max_err;
-            rep->final_dt = p->dt;
-            return LLG_OK;
-        };
-        auto advance = [&](int64_t n_accept, bool* ok) -> int {
-            int64_t target = accepted + std::max<int64_t>(n_accept, 1);
-            *ok = true;
-            while (accepted < target) {
-                if (accepted >= max_acc) {
-                    *ok = false;
-                    return LLG_OK;
-                }
-                double eps, dtu;
-                int32_t acc = 0;
-                int r = step(KIND_RK23, p, fmask, max_err, st->headroom, st->dt_min, st->dt_max, &eps, &acc, &dtu);
-                if (r) return r;
-                if (acc) {
-                    ++accepted;
-                    std::memcpy(torque_cache, h_state->red, sizeof(torque_cache));
-                } else {
-                    ++rejected;
-                }
-            }
-            return LLG_OK;
-        };
-        auto torque_now = [&](int met, double* out) -> int {
-            ++checks;
-            if (last_b_eff_valid) {
-                StepState tmp;
-                std::memcpy(tmp.red, torque_cache, sizeof(torque_cache));
-                *out = metric_from(tmp, met);
-                return LLG_OK;
-            }
-            ++rebuilds;
-            return torque_metric(p, fmask, met, out);
-        };
-        auto total_energy = [&](double* e) -> int {
-            llg_energy_breakdown b;
-            int r = energy(p->b_ext, &b);
-            *e = b.exchange + b.anisotropy + b.zeeman + b.dmi + b.demag;
-            return r;
-        };
-        bool ok;
-        if (phase1) {
-            double e0, e1;
-            if ((rc = total_energy(&e0))) return rc;
-            for (;;) {
-                if ((rc = advance(energy_stride, &ok))) return rc;
-                if (!ok) return finish(0);
-                if ((rc = total_energy(&e1))) return rc;
-                double tol = st->rel_energy_tol * std::max(std::fabs(e0), 1e-30);
-                if (e1 < e0 - tol) {
-                    e0 = e1;
-                    continue;
-                }
-                break;
-            }
-        }
-        if (!phase2) return finish(1);
-        const bool plateau_enabled = !has_thr && plateau_checks > 0;
-        const int64_t need_fails = std::max<int64_t>(plateau_checks, 1);
-        for (;;) {
-            double t_prev;
-            if ((rc = torque_now(metric, &t_prev))) return rc;
-            const bool f32mode = plateau_enabled && metric == LLG_TORQUE_MEANSQ && plateau_rel == 0.0 &&
-                                 plateau_abs == 0.0 && plateau_checks == 1 && plateau_min_checks == 1;
-            const double nf = (double)n;
-            float t_prev_f32 = f32mode ? (float)(t_prev * nf) : (float)t_prev;
-            int64_t fails = 0, comparisons = 0;
-            for (;;) {
-                if (has_thr && t_prev <= thr) {
-                    last_stage = 0;
-                    break;
-                }
-                if (plateau_enabled && fails >= need_fails) {
-                    last_stage = 1;
-                    break;
-                }
-                if (accepted >= max_acc) {
-                    last_stage = 2;
-                    has_ft = true;
-                    ft = t_prev;
-                    return finish(0);
-                }
-                if ((rc = advance(check_stride, &ok))) return rc;
-                if (!ok) {
-                    last_stage = 2;
-                    has_ft = true;
-                    ft = t_prev;
-                    return finish(0);
-                }
-                double t_new;
-                if ((rc = torque_now(metric, &t_new))) return rc;
-                if (plateau_enabled) {
-                    ++comparisons;
-                    if (comparisons < plateau_min_checks) {
-                        fails = 0;
-                    } else if (f32mode) {
-                        float t_new_f32 = (float)(t_new * nf);
-                        bool improved = t_new_f32 < t_prev_f32;
-                        t_prev_f32 = t_new_f32;
-                        fails = improved ? 0 : fails + 1;
-                    } else {
-                        double need = std::max(plateau_rel * std::max(std::fabs(t_prev), 1e-30), plateau_abs);
-                        fails = (t_prev - t_new) > need ? 0 : fails + 1;
-                    }
-                }
-                t_prev = t_new;
-            }
-            has_ft = true;
-            ft = t_prev;
-            if (max_err <= st->tighten_floor) break;
-            max_err *= st->tighten_factor;
-            if (max_err < st->tighten_floor) max_err = st->tighten_floor;
-        }
-        if ((rc = torque_now(LLG_TORQUE_MAX, &ftm))) return rc;
-        has_ftm = true;
-        const bool has_gate = st->has_final_torque_gate != 0, has_gmax = st->has_final_torque_gate_max != 0;
-        if ((has_gate || has_gmax) && st->gate_max_extra_accepted_steps > 0) {
-            const int64_t start = accepted;
-            double last_t = has_ft ? ft : INFINITY;
-            int64_t gfails = 0;
-            for (;;) {
-                double t_metric, t_max = NAN;
-                if ((rc = torque_now(metric, &t_metric))) return rc;
-                if (has_gmax || metric == LLG_TORQUE_MAX) {
-                    if (metric == LLG_TORQUE_MAX) t_max = t_metric;
-                    else if ((rc = torque_now(LLG_TORQUE_MAX, &t_max))) return rc;
-                }
-                const bool okm = !has_gate || t_metric <= st->final_torque_gate;
-                const bool okx = !has_gmax || t_max <= st->final_torque_gate_max;
-                has_ft = true;
-                ft = t_metric;
-                if (std::isfinite(t_max)) {
-                    has_ftm = true;
-                    ftm = t_max;
-                }
-                if (okm && okx) break;
-                if (accepted - start >= st->gate_max_extra_accepted_steps) return finish(3);
-                if (st->gate_plateau_fails > 0) {
-                    double need = std::max(plateau_rel * std::max(std::fabs(last_t), 1e-30), plateau_abs);
-                    gfails = (last_t - t_metric) > need ? 0 : gfails + 1;
-                    if (gfails >= st->gate_plateau_fails) return finish(3);
-                    last_t = t_metric;
-                }
-                if ((rc = advance(check_stride, &ok))) return rc;
-                if (!ok) {
-                    last_stage = 2;
-                    return finish(0);
-                }
-            }
-        }
-        return finish(2);
     }
 };
 
@@ -1149,8 +1166,15 @@ struct llg_solver {
     std::unique_ptr<llg::EngineBase> eng;
     int device;
 };
+struct llg_batch {
+    std::unique_ptr<llg::EngineBase> eng;
+    int device;
+};
 
 using llg::set_error;
+
+// Lets other translation units report through llg_last_error().
+void llg_set_error_message(const char* msg) { llg::g_last_error = msg ? msg : ""; }
 
 namespace {
 int check_device(int device) {
@@ -1164,16 +1188,36 @@ int check_device(int device) {
                                            prop.major, prop.minor);
     return LLG_OK;
 }
-int bind(llg_solver* s) {
-    if (!s || !s->eng) return set_error(LLG_ERR_INVALID, "null solver");
+template <typename H>
+int bind(H* s) {
+    if (!s || !s->eng) return set_error(LLG_ERR_INVALID, "null handle");
     cudaError_t e = cudaSetDevice(s->device);
     if (e != cudaSuccess) return set_error(LLG_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
     return LLG_OK;
 }
+int check_grid(const llg_grid* g) {
+    if (g->nx < 1 || g->ny < 1 || g->nx > 4096 || g->ny > 4096)
+        return set_error(LLG_ERR_INVALID, "grid %lldx%lld out of range [1, 4096]", (long long)g->nx, (long long)g->ny);
+    if (!(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0)) return set_error(LLG_ERR_INVALID, "cell sizes must be > 0");
+    return LLG_OK;
+}
+int make_engine(int device, int n, const llg_grid* g, const llg_material* m, int32_t precision,
+                const uint8_t* const* masks, std::unique_ptr<llg::EngineBase>* out) {
+    if (precision != LLG_PREC_FP32 && precision != LLG_PREC_FP64) return set_error(LLG_ERR_INVALID, "bad precision");
+    for (int f = 0; f < n; ++f) {
+        int rc = check_grid(&g[f]);
+        if (rc) return rc;
+    }
+    if (precision == LLG_PREC_FP32) {
+        auto* e = new llg::Engine<float>();
+        out->reset(e);
+        return e->init(device, n, g, m, masks);
+    }
+    auto* e = new llg::Engine<double>();
+    out->reset(e);
+    return e->init(device, n, g, m, masks);
+}
 }  // namespace
-
-// Lets other translation units report through llg_last_error().
-void llg_set_error_message(const char* msg) { llg::g_last_error = msg ? msg : ""; }
 
 extern "C" {
 
@@ -1201,23 +1245,10 @@ int llg_ctx_destroy(llg_ctx* ctx) {
 int llg_solver_create(llg_ctx* ctx, const llg_grid* grid, const llg_material* mat, int32_t precision,
                       const uint8_t* geom_mask, llg_solver** out) {
     if (!ctx || !grid || !mat || !out) return set_error(LLG_ERR_INVALID, "null argument");
-    if (grid->nx < 1 || grid->ny < 1 || grid->nx > 4096 || grid->ny > 4096)
-        return set_error(LLG_ERR_INVALID, "grid %lldx%lld out of range [1, 4096]", (long long)grid->nx,
-                         (long long)grid->ny);
-    if (!(grid->dx > 0) || !(grid->dy > 0) || !(grid->dz > 0)) return set_error(LLG_ERR_INVALID, "cell sizes must be > 0");
-    if (precision != LLG_PREC_FP32 && precision != LLG_PREC_FP64) return set_error(LLG_ERR_INVALID, "bad precision");
     std::unique_ptr<llg_solver> s(new llg_solver());
     s->device = ctx->device;
-    int rc;
-    if (precision == LLG_PREC_FP32) {
-        auto* e = new llg::Engine<float>();
-        s->eng.reset(e);
-        rc = e->init(ctx->device, grid, mat, geom_mask);
-    } else {
-        auto* e = new llg::Engine<double>();
-        s->eng.reset(e);
-        rc = e->init(ctx->device, grid, mat, geom_mask);
-    }
+    const uint8_t* masks[1] = {geom_mask};
+    int rc = make_engine(ctx->device, 1, grid, mat, precision, masks, &s->eng);
     if (rc) return rc;
     *out = s.release();
     return LLG_OK;
@@ -1241,12 +1272,12 @@ int llg_solver_sync(llg_solver* s) {
 int llg_set_state(llg_solver* s, const double* m) {
     int rc = bind(s);
     if (!rc && !m) rc = set_error(LLG_ERR_INVALID, "null m");
-    return rc ? rc : s->eng->set_state(m);
+    return rc ? rc : s->eng->set_state(0, m);
 }
 int llg_get_state(llg_solver* s, double* m) {
     int rc = bind(s);
     if (!rc && !m) rc = set_error(LLG_ERR_INVALID, "null m");
-    return rc ? rc : s->eng->get_state(m);
+    return rc ? rc : s->eng->get_state(0, m);
 }
 int llg_mean_m(llg_solver* s, double out3[3]) {
     int rc = bind(s);
@@ -1255,12 +1286,12 @@ int llg_mean_m(llg_solver* s, double out3[3]) {
 int llg_build_h_eff(llg_solver* s, const llg_params* p, int32_t fmask, double* b) {
     int rc = bind(s);
     if (!rc && (!p || !b)) rc = set_error(LLG_ERR_INVALID, "null argument");
-    return rc ? rc : s->eng->build_h_eff(p, fmask, b);
+    return rc ? rc : s->eng->build_h_eff(0, p, fmask, b);
 }
 int llg_compute_demag_field(llg_solver* s, double* b) {
     int rc = bind(s);
     if (!rc && !b) rc = set_error(LLG_ERR_INVALID, "null argument");
-    return rc ? rc : s->eng->demag_field(b);
+    return rc ? rc : s->eng->demag_field(0, b);
 }
 int llg_step_rk45(llg_solver* s, llg_params* p, int32_t fmask, double max_err, double headroom, double dt_min,
                   double dt_max, double* eps, int32_t* acc, double* dtu) {
@@ -1286,7 +1317,10 @@ int llg_run_rk45(llg_solver* s, llg_params* p, int32_t fmask, double max_err, do
 int llg_relax(llg_solver* s, llg_params* p, int32_t fmask, llg_relax_settings* st, llg_relax_report* rep) {
     int rc = bind(s);
     if (!rc && (!p || !st || !rep)) rc = set_error(LLG_ERR_INVALID, "null argument");
-    return rc ? rc : s->eng->relax(p, fmask, st, rep);
+    if (rc) return rc;
+    rc = s->eng->relax(p, fmask, st, rep);
+    if (!rc) st->max_err = rep->final_max_err;  // written back as relax_with_report does
+    return rc;
 }
 void llg_default_relax_settings(llg_relax_settings* st) {
     std::memset(st, 0, sizeof(*st));
@@ -1323,9 +1357,8 @@ int llg_torque_metric(llg_solver* s, const llg_params* p, int32_t fmask, int32_t
 int llg_demag_kernel_kspace(llg_solver* s, double* out) {
     int rc = bind(s);
     if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");
-    return rc ? rc : s->eng->kernel_kspace(out);
+    return rc ? rc : s->eng->kernel_kspace(0, out);
 }
-
 int llg_profile_stage(llg_solver* s, const llg_params* p, int32_t fmask, int32_t reps, double* ms3) {
     int rc = bind(s);
     if (!rc && (!p || !ms3 || reps < 1)) rc = set_error(LLG_ERR_INVALID, "bad argument");
@@ -1336,6 +1369,77 @@ int llg_solver_launch_count(llg_solver* s, int64_t* out) {
     if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");
     if (rc) return rc;
     *out = s->eng->launch_count();
+    return LLG_OK;
+}
+
+// ---------------- batches of independent films ----------------
+int llg_batch_create(llg_ctx* ctx, int32_t n, const llg_grid* grids, const llg_material* mats, int32_t precision,
+                     const uint8_t* const* masks, llg_batch** out) {
+    if (!ctx || !grids || !mats || !out || n < 1) return set_error(LLG_ERR_INVALID, "bad argument");
+    std::unique_ptr<llg_batch> b(new llg_batch());
+    b->device = ctx->device;
+    int rc = make_engine(ctx->device, n, grids, mats, precision, masks, &b->eng);
+    if (rc) return rc;
+    *out = b.release();
+    return LLG_OK;
+}
+int llg_batch_destroy(llg_batch* b) {
+    if (!b) return LLG_OK;
+    if (b->eng) cudaSetDevice(b->device);
+    delete b;
+    return LLG_OK;
+}
+int llg_batch_set_stream(llg_batch* b, void* stream) {
+    int rc = bind(b);
+    return rc ? rc : b->eng->set_stream(reinterpret_cast<cudaStream_t>(stream));
+}
+int llg_batch_set_state(llg_batch* b, int32_t film, const double* m) {
+    int rc = bind(b);
+    if (!rc && (!m || film < 0 || film >= b->eng->nfilms())) rc = set_error(LLG_ERR_INVALID, "bad film or null m");
+    return rc ? rc : b->eng->set_state(film, m);
+}
+int llg_batch_get_state(llg_batch* b, int32_t film, double* m) {
+    int rc = bind(b);
+    if (!rc && (!m || film < 0 || film >= b->eng->nfilms())) rc = set_error(LLG_ERR_INVALID, "bad film or null m");
+    return rc ? rc : b->eng->get_state(film, m);
+}
+int llg_batch_mean_m(llg_batch* b, double* out) {
+    int rc = bind(b);
+    if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc : b->eng->mean_m(out);
+}
+int llg_batch_step_rk45(llg_batch* b, llg_params* params, int32_t fmask, double max_err, double headroom,
+                        double dt_min, double dt_max, double* eps, int32_t* accepted, double* dt_used) {
+    int rc = bind(b);
+    if (!rc && (!params || !eps || !accepted || !dt_used)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc
+              : b->eng->step(llg::KIND_RK45, params, fmask, max_err, headroom, dt_min, dt_max, eps, accepted, dt_used);
+}
+int llg_batch_run_rk45(llg_batch* b, llg_params* params, int32_t fmask, double max_err, double headroom,
+                       double dt_min, double dt_max, int64_t n_accepted, double t_end, int64_t max_attempts,
+                       int64_t* accepted, int64_t* rejected, double* t) {
+    int rc = bind(b);
+    if (!rc && (!params || !accepted || !rejected || !t)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc
+              : b->eng->run(llg::KIND_RK45, params, fmask, max_err, headroom, dt_min, dt_max, n_accepted, t_end,
+                            max_attempts, accepted, rejected, t);
+}
+int llg_batch_relax(llg_batch* b, llg_params* params, int32_t fmask, const llg_relax_settings* settings,
+                    llg_relax_report* reports) {
+    int rc = bind(b);
+    if (!rc && (!params || !settings || !reports)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc : b->eng->relax(params, fmask, settings, reports);
+}
+int llg_batch_compute_energy(llg_batch* b, const double* b_ext, llg_energy_breakdown* out) {
+    int rc = bind(b);
+    if (!rc && (!b_ext || !out)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc : b->eng->energy(b_ext, out);
+}
+int llg_batch_launch_count(llg_batch* b, int64_t* out) {
+    int rc = bind(b);
+    if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");
+    if (rc) return rc;
+    *out = b->eng->launch_count();
     return LLG_OK;
 }
 

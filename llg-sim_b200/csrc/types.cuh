@@ -29,6 +29,8 @@ enum KBuf : int { KB_NONE = 0, KB_K1 = 1, KB_K2, KB_K3, KB_K4, KB_K5, KB_K6, KB_
 
 enum RhsMode : int { RHS_LLG = 0, RHS_RELAX = 1, RHS_FIELD = 2, RHS_ENERGY = 3, RHS_TORQUE = 4 };
 enum ErrMode : int { ERR_NONE = 0, ERR_RK45 = 1, ERR_RK23 = 2 };
+// Requests of the device-side relax controller.
+enum ReqKind : int { REQ_NONE = 0, REQ_ENERGY = 1, REQ_TORQUE = 2, REQ_STEP = 3 };
 
 // Slots of the per-block FP64 partial reductions.
 enum RedSlot : int {
@@ -54,6 +56,7 @@ struct StepState {
     int active;
     int err_code;
     int order;                    // 5 for RK45, 3 for RK23 (controller exponent 1/order)
+    int req;                      // request of the device relax controller (ReqKind)
     double red[RED_NSLOT];        // finalised reductions of the last reduction pass
 };
 
@@ -107,6 +110,7 @@ struct EvalSpec {
     int local;                    // include the local terms (0: demag field only)
     int skip_if_fsal;             // skip when the film's FSAL torque is valid
     int reduce;                   // write per-block reductions (torque / energy / mean m)
+    int req;                      // run only for films whose StepState::req equals this (0: always)
     // Error-norm weights over k1..k7: wb = solution weights b_q, wh = embedded
     // weights bhat_q (RK45: torques, llg.rs:948-997; RK23: states, llg.rs:356-401)
     double wb[8];

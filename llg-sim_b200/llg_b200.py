@@ -136,6 +136,19 @@ def lib():
             "llg_profile_stage": (C.c_int, [vp, P(_Params), i32, i32, dp]),
             "llg_solver_launch_count": (C.c_int, [vp, P(i64)]),
             "llg_demag_field_noalloc": (C.c_int, [i64, i64, C.c_double, vp, vp, vp, vp]),
+            "llg_batch_create": (C.c_int, [vp, i32, P(_Grid), P(_Material), i32, P(C.c_void_p), P(vp)]),
+            "llg_batch_destroy": (C.c_int, [vp]),
+            "llg_batch_set_stream": (C.c_int, [vp, vp]),
+            "llg_batch_set_state": (C.c_int, [vp, i32, dp]),
+            "llg_batch_get_state": (C.c_int, [vp, i32, dp]),
+            "llg_batch_mean_m": (C.c_int, [vp, dp]),
+            "llg_batch_step_rk45": (C.c_int, [vp, P(_Params), i32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              dp, P(i32), dp]),
+            "llg_batch_run_rk45": (C.c_int, [vp, P(_Params), i32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                             i64, C.c_double, i64, P(i64), P(i64), dp]),
+            "llg_batch_relax": (C.c_int, [vp, P(_Params), i32, P(RelaxSettings), P(RelaxReport)]),
+            "llg_batch_compute_energy": (C.c_int, [vp, dp, P(EnergyBreakdown)]),
+            "llg_batch_launch_count": (C.c_int, [vp, P(i64)]),
             "llg_init_random": (None, [i64, C.c_uint64, dp]),
             "llg_init_uniform_with_noise": (None, [i64, dp, C.c_double, C.c_uint64, dp]),
         }
@@ -350,6 +363,106 @@ class Solver:
         out = np.empty(4 * (self.grid.nx + 1) * (self.grid.ny + 1))
         _check(lib().llg_demag_kernel_kspace(self.h, _dp(out)))
         return out.reshape(4, self.grid.ny + 1, self.grid.nx + 1)
+
+
+class Batch:
+    """Independent films of possibly different sizes advanced together: one launch
+    per pass over all films, per-film dt and acceptance, device-side relax."""
+
+    def __init__(self, grids, materials, precision=FP32, masks=None, device=0):
+        self.n = len(grids)
+        self.grids, self.materials, self.precision = list(grids), list(materials), precision
+        G = (_Grid * self.n)(*[g._c() for g in grids])
+        M = (_Material * self.n)(*[m._c() for m in materials])
+        self._masks = []
+        mp = None
+        if masks is not None:
+            arr = (C.c_void_p * self.n)()
+            for i, mk in enumerate(masks):
+                if mk is None:
+                    arr[i] = None
+                else:
+                    a = np.ascontiguousarray(np.asarray(mk).reshape(-1).astype(np.uint8))
+                    self._masks.append(a)
+                    arr[i] = a.ctypes.data_as(C.c_void_p)
+            mp = arr
+        h = C.c_void_p()
+        _check(lib().llg_batch_create(_ctx(device), self.n, G, M, int(precision), mp, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().llg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        _check(lib().llg_batch_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_state(self, f, m):
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        assert m.size == 3 * self.grids[f].n_cells()
+        _check(lib().llg_batch_set_state(self.h, int(f), _dp(m)))
+
+    def get_state(self, f):
+        out = np.empty((self.grids[f].n_cells(), 3))
+        _check(lib().llg_batch_get_state(self.h, int(f), _dp(out)))
+        return out
+
+    def mean_m(self):
+        out = np.empty((self.n, 3))
+        _check(lib().llg_batch_mean_m(self.h, _dp(out)))
+        return out
+
+    def _params(self, params):
+        assert len(params) == self.n
+        return (_Params * self.n)(*[p._c() for p in params])
+
+    def step_rk45(self, params, field_mask, max_err, headroom, dt_min, dt_max):
+        P = self._params(params)
+        eps, dtu = np.empty(self.n), np.empty(self.n)
+        acc = (C.c_int32 * self.n)()
+        _check(lib().llg_batch_step_rk45(self.h, P, int(field_mask), float(max_err), float(headroom), float(dt_min),
+                                         float(dt_max), _dp(eps), acc, _dp(dtu)))
+        for i, p in enumerate(params):
+            p.dt = P[i].dt
+        return eps, np.array(acc[:], dtype=bool), dtu
+
+    def run_rk45(self, params, field_mask, max_err, headroom, dt_min, dt_max, n_accepted=-1, t_end=float("inf"),
+                 max_attempts=-1):
+        P = self._params(params)
+        a, r = (C.c_int64 * self.n)(), (C.c_int64 * self.n)()
+        t = np.empty(self.n)
+        _check(lib().llg_batch_run_rk45(self.h, P, int(field_mask), float(max_err), float(headroom), float(dt_min),
+                                        float(dt_max), int(n_accepted), float(t_end), int(max_attempts), a, r,
+                                        _dp(t)))
+        for i, p in enumerate(params):
+            p.dt = P[i].dt
+        return np.array(a[:]), np.array(r[:]), t
+
+    def relax(self, params, field_mask, settings):
+        P = self._params(params)
+        reps = (RelaxReport * self.n)()
+        _check(lib().llg_batch_relax(self.h, P, int(field_mask), C.byref(settings), reps))
+        for i, p in enumerate(params):
+            p.dt = P[i].dt
+        return list(reps)
+
+    def compute_energy(self, b_exts):
+        be = np.ascontiguousarray(np.asarray(b_exts, dtype=np.float64).reshape(self.n, 3))
+        out = (EnergyBreakdown * self.n)()
+        _check(lib().llg_batch_compute_energy(self.h, _dp(be), out))
+        return list(out)
+
+    def launch_count(self):
+        out = C.c_int64()
+        _check(lib().llg_batch_launch_count(self.h, C.byref(out)))
+        return out.value
 
 
 def demag_field_noalloc(nx, ny, ms, m_dev_ptr, kernel_planes_dev_ptr, b_dev_ptr, stream_ptr=0):

@@ -1,0 +1,159 @@
+"""Batched films and the device-side relax controller, against the FP64 oracle."""
+import numpy as np
+import pytest
+
+from helpers import GAMMA, case, gpu_solver, holes_mask, oracle_solver, random_m, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_objs(gpu, c):
+    g = gpu.Grid2D(c["nx"], c["ny"], c["dx"], c["dy"], c["dz"])
+    m = gpu.Material(c["ms"], c["a_ex"], c["k_u"], c["easy"], c["dmi"], c["demag"])
+    return g, m
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+def test_relax_matches_oracle(orc, gpu, prec):
+    """relax_with_report: phase-1 energy descent, threshold stages, tightening."""
+    nx, ny = 16, 12
+    c = case(nx, ny)
+    o = oracle_solver(orc, c)
+    g = gpu_solver(gpu, c, prec)
+    m = orc.init_random(nx * ny, 4)
+    g.set_state(m)
+    mo = m.copy()
+    bext = (0.05, 0.0, 0.0)
+    po = orc.make_params(GAMMA, 0.5, 1e-13, bext)
+    pg = gpu.LLGParams(GAMMA, 0.5, 1e-13, bext)
+    kw = dict(torque_threshold=1e-3, max_accepted_steps=20000)
+    so = orc.default_relax_settings(**kw)
+    sg = gpu.RelaxSettings.default(**kw)
+    ro = o.relax(mo, po, 2, so)
+    rg = g.relax(pg, 2, sg)
+    assert rg.stop_reason == ro.stop_reason == 2
+    assert rg.last_stage_stop == ro.last_stage_stop
+    assert rg.final_torque_max <= 1e-3
+    if prec == 1:
+        assert (rg.accepted_steps, rg.rejected_steps, rg.torque_checks, rg.torque_field_rebuilds) == \
+            (ro.accepted_steps, ro.rejected_steps, ro.torque_checks, ro.torque_field_rebuilds)
+        assert rg.final_torque_max == pytest.approx(ro.final_torque_max, rel=1e-6)
+        assert np.abs(g.get_state() - mo).max() < 1e-9
+        assert sg.max_err == pytest.approx(so.max_err)
+        eo = o.energy(mo, bext)
+        eg = g.compute_energy(bext)
+        assert eg.total() == pytest.approx(eo.total(), rel=1e-9)
+    else:
+        # FP32 rounding changes the descent path (a different number of steps to reach the
+        # threshold), so the FP32 result is checked as a relaxed state: the FP64 oracle
+        # evaluated at the GPU's final m sees torque below the threshold (FP32 field error
+        # allowance 2 %), the GPU energy equals the oracle's energy of that state, and the
+        # state sits in the same minimum as the oracle's relaxed state.
+        mg = g.get_state()
+        b = o.build_h_eff(mg, bext)
+        assert orc.torque_metric(mg, b, orc.TORQUE_MAX) <= 1.02e-3
+        eg = g.compute_energy(bext)
+        assert eg.total() == pytest.approx(o.energy(mg, bext).total(), rel=1e-5)
+        assert eg.total() == pytest.approx(o.energy(mo, bext).total(), rel=1e-3)
+        assert np.abs(mg - mo).max() < 0.05
+
+
+def test_relax_plateau_mode_matches_oracle(orc, gpu):
+    """MuMax-like plateau settings (mumax_like_relax_settings, relax.rs:787-808), phase-1 cap."""
+    nx, ny = 16, 12
+    c = case(nx, ny)
+    o = oracle_solver(orc, c)
+    g = gpu_solver(gpu, c, gpu.FP64)
+    m = orc.init_random(nx * ny, 4)
+    g.set_state(m)
+    mo = m.copy()
+    kw = dict(torque_threshold=None, torque_metric=3, torque_plateau_checks=1, torque_plateau_min_checks=1,
+              torque_plateau_rel=0.0, torque_plateau_abs=0.0, rel_energy_tol=1e-9, max_accepted_steps=3000)
+    so = orc.default_relax_settings(**kw)
+    sg = gpu.RelaxSettings.default(**kw)
+    po = orc.make_params(GAMMA, 0.5, 1e-13, (0, 0, 0.01))
+    pg = gpu.LLGParams(GAMMA, 0.5, 1e-13, (0, 0, 0.01))
+    ro = o.relax(mo, po, 2, so)
+    rg = g.relax(pg, 2, sg)
+    assert (rg.stop_reason, rg.last_stage_stop, rg.accepted_steps, rg.rejected_steps, rg.torque_checks) == \
+        (ro.stop_reason, ro.last_stage_stop, ro.accepted_steps, ro.rejected_steps, ro.torque_checks)
+    # identical decisions over thousands of steps; FP64 round-off (FFT order) accumulates to ~1e-8
+    assert np.abs(g.get_state() - mo).max() < 1e-7
+
+
+def test_batch_mixed_sizes_rk45_matches_oracle(orc, gpu):
+    """Films of uneven sizes in one batch, each with its own dt sequence."""
+    shapes = [(12, 10), (16, 8), (7, 5), (20, 12)]
+    cases = [case(nx, ny, ms=6e5 + 1e5 * i, a_ex=1.0e-11 + 1e-12 * i) for i, (nx, ny) in enumerate(shapes)]
+    gs, ms = zip(*[_gpu_objs(gpu, c) for c in cases])
+    b = gpu.Batch(gs, ms, gpu.FP64)
+    m0 = [orc.init_uniform_with_noise(c["nx"] * c["ny"], (1, 0, 0), 0.2, 50 + i) for i, c in enumerate(cases)]
+    for i, m in enumerate(m0):
+        b.set_state(i, m)
+    fields = [(0.01 * (i + 1), 0.005, 0.0) for i in range(len(cases))]
+    pg = [gpu.LLGParams(GAMMA, 0.02, 1e-13, f) for f in fields]
+    acc, rej, t = b.run_rk45(pg, 2, 1e-5, 0.8, 1e-19, 1e-11, t_end=2e-11)
+    for i, c in enumerate(cases):
+        o = oracle_solver(orc, c)
+        mo = m0[i].copy()
+        po = orc.make_params(GAMMA, 0.02, 1e-13, fields[i])
+        tt, a, r = 0.0, 0, 0
+        while tt + 1e-18 < 2e-11:
+            po.dt = min(po.dt, 2e-11 - tt)
+            _, ok, dtu = o.step_rk45(mo, po, 2, 1e-5, 0.8, 1e-19, 1e-11)
+            if ok:
+                tt += dtu
+                a += 1
+            else:
+                r += 1
+        assert (acc[i], rej[i]) == (a, r), i
+        assert t[i] == pytest.approx(2e-11, rel=1e-12)
+        assert np.abs(b.get_state(i) - mo).max() < 1e-10, i
+
+
+def test_batch_relax_with_masks_matches_single_films(orc, gpu):
+    """Batched device relax of masked films equals relaxing each film alone (FP64)."""
+    nx, ny = 32, 32
+    masks = [holes_mask(nx, ny, [(4, 2, 6)]), None, holes_mask(nx, ny, [(-6, 5, 5), (7, -7, 4)])]
+    dmis = [1e-3, None, 2e-3]
+    cases = [case(nx, ny, dmi=dmis[i], mask=masks[i]) for i in range(3)]
+    gs, ms = zip(*[_gpu_objs(gpu, c) for c in cases])
+    b = gpu.Batch(gs, ms, gpu.FP64, masks=masks)
+    m0 = [random_m(orc, nx * ny, 70 + i, masks[i]) for i in range(3)]
+    for i in range(3):
+        b.set_state(i, m0[i])
+    fields = [(0.01, 0.0, 0.0), (0.0, 0.02, 0.0), (0.015, 0.01, 0.0)]
+    st = gpu.RelaxSettings.default(torque_threshold=1e-3, max_accepted_steps=20000)
+    reps = b.relax([gpu.LLGParams(GAMMA, 0.5, 1e-13, f) for f in fields], 2, st)
+    energies = b.compute_energy(fields)
+    for i in range(3):
+        o = oracle_solver(orc, cases[i])
+        mo = m0[i].copy()
+        ro = o.relax(mo, orc.make_params(GAMMA, 0.5, 1e-13, fields[i]), 2, orc.default_relax_settings(
+            torque_threshold=1e-3, max_accepted_steps=20000))
+        assert (reps[i].stop_reason, reps[i].accepted_steps, reps[i].rejected_steps) == \
+            (ro.stop_reason, ro.accepted_steps, ro.rejected_steps), i
+        mg = b.get_state(i)
+        assert np.abs(mg - mo).max() < 1e-7, i  # FP64 round-off over thousands of steps
+        if masks[i] is not None:
+            assert np.all(mg[masks[i] == 0] == 0.0)
+        eo = o.energy(mo, fields[i])
+        assert energies[i].total() == pytest.approx(eo.total(), rel=1e-9)
+
+
+def test_batch_shared_shape_uses_register_fft(orc, gpu):
+    """A batch of same-shape power-of-two films runs the register-FFT kernels."""
+    c = case(64, 32)
+    g, m = _gpu_objs(gpu, c)
+    b = gpu.Batch([g] * 3, [m] * 3, gpu.FP32)
+    for i in range(3):
+        b.set_state(i, orc.init_random(64 * 32, 100 + i))
+    pg = [gpu.LLGParams(GAMMA, 0.3, 1e-13, (0, 0, 0.01 * i)) for i in range(3)]
+    acc, rej, t = b.run_rk45(pg, 2, 1e-5, 0.8, 1e-19, 1e-11, n_accepted=10)
+    assert list(acc) == [10, 10, 10]
+    for i in range(3):
+        s = gpu_solver(gpu, c, gpu.FP32)
+        s.set_state(orc.init_random(64 * 32, 100 + i))
+        p = gpu.LLGParams(GAMMA, 0.3, 1e-13, (0, 0, 0.01 * i))
+        s.run_rk45(p, 2, 1e-5, 0.8, 1e-19, 1e-11, n_accepted=10)
+        assert np.abs(s.get_state() - b.get_state(i)).max() < 1e-6
