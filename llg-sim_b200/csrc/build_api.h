@@ -21,8 +21,6 @@ cudaError_t launch_fft_strided(void* data, int L, const void* tw2, long long ele
 cudaError_t build_demag_kernel(int nx, int ny, double dx, double dy, double dz, bool fp64_out, void* khat_out,
                                double* k64_out_dev, cudaStream_t s);
 
-// Per-parity unfolded kernel table for the register-FFT column pass.
-cudaError_t build_kernel_parity(int nx, int ny, bool fp64, const void* khat, void* kpar, cudaStream_t s);
 
 // Launch geometry of one film set.
 struct LaunchGeom {
@@ -33,7 +31,9 @@ struct LaunchGeom {
     int n_col_items;
     size_t smem_row;
     size_t smem_col;
-    int grid_row;
+    int grid_row;     // row-forward pass (and generic row kernels)
+    int grid_rinv;    // register-FFT row-inverse pass, lean epilogue
+    int grid_rfull;   // register-FFT row-inverse pass, full epilogue
     int grid_col;
     bool any_demag;
     int fast_row;     // register-FFT row kernels for L = nx (0: generic kernels)
@@ -54,7 +54,8 @@ template <typename R>
 FastCfg fast_config(int nx, int ny);
 // Resident blocks per SM of the fast kernels (after prepare_eval_kernels).
 template <typename R>
-void fast_occupancy(int nx, int ny, int* row_blocks_per_sm, int* col_blocks_per_sm);
+void fast_occupancy(int nx, int ny, int* fwd_blocks_per_sm, int* inv_blocks_per_sm, int* full_blocks_per_sm,
+                    int* col_blocks_per_sm);
 template <typename R>
 cudaError_t build_pass_tables(void* out_row, int nx, void* out_col, int ny, cudaStream_t s);
 

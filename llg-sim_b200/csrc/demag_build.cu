@@ -153,36 +153,6 @@ __global__ void k_kernel_extract(int nx, int ny, const cx<double>* __restrict__ 
 
 }  // namespace
 
-// Per-parity unfolded copy of the kernel planes for the register-FFT column
-// pass: Kpar[kx][p][k'] = Khat(kx, ky = 2k'+p) with ky folded onto [0, ny] and
-// the odd-in-ky sign of Kxy applied, so that each transform group reads its
-// kernel values contiguously.
-template <typename R>
-__global__ void k_kernel_parity(int nx, int ny, const r4<R>* __restrict__ khat, r4<R>* __restrict__ kpar) {
-    const long long total = (long long)(nx + 1) * 2 * ny;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int kp = (int)(e % ny);
-        const int par = (int)((e / ny) % 2);
-        const int kx = (int)(e / (2LL * ny));
-        const int ky = 2 * kp + par;
-        const int kyf = ky <= ny ? ky : 2 * ny - ky;
-        r4<R> k = khat[(long long)kx * (ny + 1) + kyf];
-        if (ky > ny) k.y = -k.y;
-        kpar[e] = k;
-    }
-}
-
-cudaError_t build_kernel_parity(int nx, int ny, bool fp64, const void* khat, void* kpar, cudaStream_t s) {
-    if (fp64)
-        k_kernel_parity<double><<<1184, 256, 0, s>>>(nx, ny, reinterpret_cast<const r4<double>*>(khat),
-                                                     reinterpret_cast<r4<double>*>(kpar));
-    else
-        k_kernel_parity<float><<<1184, 256, 0, s>>>(nx, ny, reinterpret_cast<const r4<float>*>(khat),
-                                                    reinterpret_cast<r4<float>*>(kpar));
-    return cudaGetLastError();
-}
-
 template <typename R>
 __global__ void k_twiddles(cx<R>* tw, int L2) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < L2; k += gridDim.x * blockDim.x) {

@@ -26,6 +26,7 @@ bool dispatch_L(int L, F&& f) {
 }
 
 constexpr size_t kSmemMax = 227 * 1024;
+constexpr size_t kStaticSmemCol = 64;   // mbarriers and the timeout flag of k_column_fast
 
 // Intermediate RK stages need only the torque: no reductions, error norm or
 // field output.
@@ -52,7 +53,7 @@ FastCfg fast_config(int nx, int ny) {
         c.smem_col = ColCfg<R, L>::SMEM;
         c.twp_col_size = TwTab<R, L>::size;
     });
-    c.ok = okr && okc && c.smem_row <= kSmemMax && c.smem_col <= kSmemMax;
+    c.ok = okr && okc && c.smem_row <= kSmemMax && c.smem_col + kStaticSmemCol <= kSmemMax;
     return c;
 }
 
@@ -97,7 +98,7 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
             cudaFuncSetAttribute(k_row_inverse_fast<R, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
         }
-        if (ColCfg<R, L>::SMEM <= kSmemMax)
+        if (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
             cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ColCfg<R, L>::SMEM);
     };
@@ -116,10 +117,10 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
                         k_row_forward_fast<R, L><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
                             g.films, g.row_items, g.n_row_items, spec);
                     else if (lean_epilogue(spec))
-                        k_row_inverse_fast<R, L, true><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                        k_row_inverse_fast<R, L, true><<<g.grid_rinv, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
                             g.films, g.row_items, g.n_row_items, spec);
                     else
-                        k_row_inverse_fast<R, L, false><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                        k_row_inverse_fast<R, L, false><<<g.grid_rfull, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
                             g.films, g.row_items, g.n_row_items, spec);
                 }
             });
@@ -132,7 +133,7 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
         if (g.fast_col) {
             dispatch_L<R>(g.fast_col, [&](auto LC) {
                 constexpr int L = decltype(LC)::value;
-                if constexpr (ColCfg<R, L>::SMEM <= kSmemMax)
+                if constexpr (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
                     k_column_fast<R, L><<<g.grid_col, ColCfg<R, L>::THREADS, ColCfg<R, L>::SMEM, s>>>(
                         g.films, g.col_items, g.n_col_items, spec);
             });
@@ -155,25 +156,27 @@ cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t 
 }
 
 template <typename R>
-void fast_occupancy(int nx, int ny, int* row_blocks_per_sm, int* col_blocks_per_sm) {
-    *row_blocks_per_sm = 1;
-    *col_blocks_per_sm = 1;
+void fast_occupancy(int nx, int ny, int* fwd_blocks_per_sm, int* inv_blocks_per_sm, int* full_blocks_per_sm,
+                    int* col_blocks_per_sm) {
+    *fwd_blocks_per_sm = *inv_blocks_per_sm = *full_blocks_per_sm = *col_blocks_per_sm = 1;
     dispatch_L<R>(nx, [&](auto LC) {
         constexpr int L = decltype(LC)::value;
         if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
             int a = 1, b = 1, c = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_row_forward_fast<R, L>, RowCfg<R, L>::THREADS,
                                                           RowCfg<R, L>::SMEM);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_row_inverse_fast<R, L, false>, RowCfg<R, L>::THREADS,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_row_inverse_fast<R, L, true>, RowCfg<R, L>::THREADS,
                                                           RowCfg<R, L>::SMEM);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_row_inverse_fast<R, L, true>, RowCfg<R, L>::THREADS,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_row_inverse_fast<R, L, false>, RowCfg<R, L>::THREADS,
                                                           RowCfg<R, L>::SMEM);
-            *row_blocks_per_sm = std::max(1, std::min(a, std::min(b, c)));
+            *fwd_blocks_per_sm = std::max(1, a);
+            *inv_blocks_per_sm = std::max(1, b);
+            *full_blocks_per_sm = std::max(1, c);
         }
     });
     dispatch_L<R>(ny, [&](auto LC) {
         constexpr int L = decltype(LC)::value;
-        if constexpr (ColCfg<R, L>::SMEM <= kSmemMax) {
+        if constexpr (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax) {
             int a = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L>, ColCfg<R, L>::THREADS,
                                                           ColCfg<R, L>::SMEM);
@@ -181,9 +184,8 @@ void fast_occupancy(int nx, int ny, int* row_blocks_per_sm, int* col_blocks_per_
         }
     });
 }
-
-template void fast_occupancy<float>(int, int, int*, int*);
-template void fast_occupancy<double>(int, int, int*, int*);
+template void fast_occupancy<float>(int, int, int*, int*, int*, int*);
+template void fast_occupancy<double>(int, int, int*, int*, int*, int*);
 template FastCfg fast_config<float>(int, int);
 template FastCfg fast_config<double>(int, int);
 template cudaError_t build_pass_tables<float>(void*, int, void*, int, cudaStream_t);

@@ -6,6 +6,7 @@
 #pragma once
 #include "field_kernels.cuh"
 #include "fft_reg.cuh"
+#include "async_copy.cuh"
 
 namespace llg {
 
@@ -19,13 +20,20 @@ struct RowCfg {
     static constexpr int NGRP = T + T / 2;
     static constexpr int NSIG = 2 * NGRP;
     static constexpr int THREADS = NSIG * G;
+    // register caps: one resident block at least (REGCAP), three resident
+    // 192-thread blocks per SM for the FP32 forward and lean inverse passes (MAXREG)
+    static constexpr int REGCAP = (65536 / THREADS) / 8 * 8 > 255 ? 255 : (65536 / THREADS) / 8 * 8;
+    static constexpr int MAXREG = (sizeof(R) == 4 && THREADS <= 192) ? 112 : REGCAP;
     static constexpr int BUF = Pad<R, L>::size;
     static constexpr int SMEM_CX = NSIG * BUF + TwTab<R, L>::size + L;
     static constexpr size_t SMEM = sizeof(cx<R>) * (size_t)SMEM_CX;
 };
 
 // Column pass: NC columns per block, six signals per column (3 components x
-// even / odd ky bins).
+// even / odd ky bins).  Shared memory: the signal exchange buffers, the pass
+// tables and pre-twiddles, and the staging areas that the bulk copies of the
+// next item's spectrum columns (Xst, [3][NC][L]) and folded kernel columns
+// (Kst, [NC][L+1]) land in while the current item is transformed.
 template <typename R, int L>
 struct ColCfg {
     using P = FPlan<R, L>;
@@ -34,8 +42,12 @@ struct ColCfg {
     static constexpr int NSIG = 6 * NC;
     static constexpr int THREADS = NSIG * G;
     static constexpr int BUF = Pad<R, L>::size;
-    static constexpr int SMEM_CX = NSIG * BUF + TwTab<R, L>::size + L;
-    static constexpr size_t SMEM = sizeof(cx<R>) * (size_t)SMEM_CX;
+    static constexpr size_t al16(size_t b) { return (b + 15) / 16 * 16; }
+    static constexpr size_t OFF_TW = al16(sizeof(cx<R>) * (size_t)NSIG * BUF);
+    static constexpr size_t OFF_PRE = al16(OFF_TW + sizeof(cx<R>) * (size_t)TwTab<R, L>::size);
+    static constexpr size_t OFF_XST = al16(OFF_PRE + sizeof(cx<R>) * (size_t)L);
+    static constexpr size_t OFF_KST = al16(OFF_XST + sizeof(cx<R>) * 3 * (size_t)NC * L);
+    static constexpr size_t SMEM = al16(OFF_KST + sizeof(r4<R>) * (size_t)NC * (L + 1));
 };
 
 template <typename R>
@@ -47,7 +59,7 @@ __device__ __forceinline__ void load_tables(cx<R>* twp, const cx<R>* __restrict_
 
 // ---------------------------------------------------------------------------
 template <typename R, int L>
-__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_forward_fast(const FilmDev* __restrict__ films,
+__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((RowCfg<R, L>::MAXREG)) k_row_forward_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
                                                                             int nitems, EvalSpec spec) {
     using C = RowCfg<R, L>;
@@ -84,34 +96,63 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_forward_fast(cons
             cq[q] = q < spec.nterm ? (R)(dt * spec.a[q]) : (R)0;
         }
         const R Ms = (R)F.ms;
-        for (int e = tid; e < T * L; e += C::THREADS) {
-            const int r = e / L, i = e - r * L, j = j0 + r;
-            R v[3] = {(R)0, (R)0, (R)0};
-            if (j < ny) {
-                const int idx = j * L + i;
-                if (spec.nterm > 0) {
-                    v[0] = m0[idx]; v[1] = m0[n + idx]; v[2] = m0[2 * n + idx];
+        // m_s = normalize(m0 + sum_q dt*a_q*k_q) in two sweeps over 16-byte vectors of
+        // W cells: (1) per component, the combination (all its loads in flight
+        // together) into the packed signal slots; (2) per cell, normalisation (or
+        // vacuum), the m_s store and the scaling by Ms.  Signal slots: x, y of row r
+        // in buffer 2r (re, im); z of rows 2p, 2p+1 in buffer 2(T+p) (re, im).
+        constexpr int W = Vec16<R>::W, NV = T * L / W;
+        auto slot = [&](int c, int r, int i) -> R* {
+            cx<R>* z = c < 2 ? &buf[(2 * r) * BUF + padi<E>(i)] : &buf[(2 * (T + r / 2)) * BUF + padi<E>(i)];
+            return (c == 0 || (c == 2 && (r & 1) == 0)) ? &z->re : &z->im;
+        };
+#pragma unroll 1
+        for (int e = tid; e < 3 * NV; e += C::THREADS) {
+            const int c = e / NV, ev = e - c * NV;
+            const int c0 = ev * W, r = c0 / L, i0 = c0 - r * L, j = j0 + r;
+            Vec16<R> a;
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) {
+            for (int l = 0; l < W; ++l) a.v[l] = (R)0;
+            if (j < ny) {
+                const int idx = c * n + j * L + i0;
+                if (spec.nterm > 0) {
+                    a = ldv(m0 + idx);
+                    Vec16<R> ka[6];
+#pragma unroll
+                    for (int q = 0; q < 6; ++q)
+                        if (q < spec.nterm) ka[q] = ldv(kp[q] + idx);
+#pragma unroll
+                    for (int q = 0; q < 6; ++q)
                         if (q < spec.nterm) {
-                            const R* k = kp[q];
-                            v[0] = v[0] + cq[q] * k[idx];
-                            v[1] = v[1] + cq[q] * k[n + idx];
-                            v[2] = v[2] + cq[q] * k[2 * n + idx];
+#pragma unroll
+                            for (int l = 0; l < W; ++l) a.v[l] = a.v[l] + cq[q] * ka[q].v[l];
                         }
-                    }
-                    if (cell_inside(F, idx)) normalize3(v);
-                    else { v[0] = (R)0; v[1] = (R)0; v[2] = (R)0; }
-                    ms[idx] = v[0]; ms[n + idx] = v[1]; ms[2 * n + idx] = v[2];
                 } else {
-                    v[0] = ms[idx]; v[1] = ms[n + idx]; v[2] = ms[2 * n + idx];
+                    a = ldv(ms + idx);
                 }
             }
-            if (do_fft) {
-                buf[(2 * r) * BUF + padi<E>(i)] = mkc(Ms * v[0], Ms * v[1]);
-                cx<R>* zp = &buf[(2 * (T + r / 2)) * BUF + padi<E>(i)];
-                if ((r & 1) == 0) zp->re = Ms * v[2];
-                else zp->im = Ms * v[2];
+#pragma unroll
+            for (int l = 0; l < W; ++l) *slot(c, r, i0 + l) = a.v[l];
+        }
+        __syncthreads();
+        for (int e = tid; e < NV; e += C::THREADS) {
+            const int c0 = e * W, r = c0 / L, i0 = c0 - r * L, j = j0 + r;
+            Vec16<R> v0, v1, v2;
+#pragma unroll
+            for (int l = 0; l < W; ++l) {
+                R a[3] = {*slot(0, r, i0 + l), *slot(1, r, i0 + l), *slot(2, r, i0 + l)};
+                if (spec.nterm > 0 && j < ny) {
+                    if (cell_inside(F, j * L + i0 + l)) normalize3(a);
+                    else { a[0] = (R)0; a[1] = (R)0; a[2] = (R)0; }
+                }
+                v0.v[l] = a[0]; v1.v[l] = a[1]; v2.v[l] = a[2];
+                *slot(0, r, i0 + l) = Ms * a[0];
+                *slot(1, r, i0 + l) = Ms * a[1];
+                *slot(2, r, i0 + l) = Ms * a[2];
+            }
+            if (spec.nterm > 0 && j < ny) {
+                const int idx = j * L + i0;
+                stv(ms + idx, v0); stv(ms + n + idx, v1); stv(ms + 2 * n + idx, v2);
             }
         }
         if (!do_fft) continue;
@@ -134,27 +175,78 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_forward_fast(cons
         __syncthreads();
         cx<R>* __restrict__ X = reinterpret_cast<cx<R>*>(F.X);
         constexpr int K1 = L + 1, L2 = 2 * L;
-        for (int e = tid; e < 3 * K1 * T; e += C::THREADS) {
-            const int r = e % T, rest = e / T;
+        // unpack the two real rows of each transform; PER consecutive rows of one
+        // (component, kx) make one 16-byte store into the column-major spectrum
+        constexpr int PER = 16 / (int)sizeof(cx<R>), TP = T / PER;
+        for (int e = tid; e < 3 * K1 * TP; e += C::THREADS) {
+            const int rp = e % TP, rest = e / TP;
             const int k = rest % K1, c = rest / K1;
-            const int j = j0 + r;
-            if (j >= ny) continue;
-            int gg, half;
-            if (c < 2) { gg = r; half = c; }
-            else { gg = T + r / 2; half = r & 1; }
+            const int r0 = rp * PER;
+            if (j0 + r0 >= ny) continue;
             const int km = (L2 - k) % L2;
-            const cx<R> zk = buf[(2 * gg + (k & 1)) * BUF + padi<E>(k >> 1)];
-            const cx<R> zm = buf[(2 * gg + (km & 1)) * BUF + padi<E>(km >> 1)];
-            cx<R> out;
-            if (half == 0) out = mkc((R)0.5 * (zk.re + zm.re), (R)0.5 * (zk.im - zm.im));
-            else out = mkc((R)0.5 * (zk.im + zm.im), (R)0.5 * (zm.re - zk.re));
-            X[(c * K1 + k) * ny + j] = out;
+            cx<R> out[PER];
+#pragma unroll
+            for (int q = 0; q < PER; ++q) {
+                const int r = r0 + q;
+                int gg, half;
+                if (c < 2) { gg = r; half = c; }
+                else { gg = T + r / 2; half = r & 1; }
+                const cx<R> zk = buf[(2 * gg + (k & 1)) * BUF + padi<E>(k >> 1)];
+                const cx<R> zm = buf[(2 * gg + (km & 1)) * BUF + padi<E>(km >> 1)];
+                if (half == 0) out[q] = mkc((R)0.5 * (zk.re + zm.re), (R)0.5 * (zk.im - zm.im));
+                else out[q] = mkc((R)0.5 * (zk.im + zm.im), (R)0.5 * (zm.re - zk.re));
+            }
+            Vec16<R> pk;
+#pragma unroll
+            for (int q = 0; q < PER; ++q) { pk.v[2 * q] = out[q].re; pk.v[2 * q + 1] = out[q].im; }
+            stv(reinterpret_cast<R*>(X + ((size_t)c * K1 + k) * ny + j0 + r0), pk);
         }
         __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
+// Column pass.  Item = NC consecutive kx columns of one film.  Per column: the
+// pruned forward y-transforms of the three components (even and odd ky bins as
+// two length-L transforms, odd ones pre-twiddled by W_{2L}^n), the product with
+// the real kernel planes (Bx = Kxx Mx + Kxy My, By = Kxy Mx + Kyy My,
+// Bz = Kzz Mz; demag_fft_uniform.rs:700-742), and the pruned inverse keeping
+// the L physical rows.  The spectrum and kernel columns of the block's next item
+// are fetched by bulk copies while this item is transformed.
+template <typename R, int L>
+__device__ __forceinline__ bool col_item_has(const FilmDev* __restrict__ films, const WorkItem* __restrict__ items,
+                                             int nitems, const EvalSpec& spec, int it) {
+    return it < nitems && spec.demag && films[items[it].film].demag_mat;
+}
+
+template <typename R, int L>
+__device__ __forceinline__ void col_issue_x(const FilmDev* __restrict__ films, const WorkItem* __restrict__ items,
+                                            int it, cx<R>* xst, uint64_t* bar) {
+    using C = ColCfg<R, L>;
+    const WorkItem w = items[it];
+    const FilmDev& F = films[w.film];
+    const int K1 = F.nx + 1, kx0 = w.blk * C::NC;
+    const int nv = min(C::NC, K1 - kx0);
+    const uint32_t bytes = (uint32_t)(sizeof(cx<R>) * (size_t)nv * L);
+    const cx<R>* X = reinterpret_cast<const cx<R>*>(F.X);
+    mbar_arrive_expect_tx(bar, 3 * bytes);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) bulk_copy_g2s(xst + (size_t)c * C::NC * L, X + ((size_t)c * K1 + kx0) * L, bytes, bar);
+}
+
+template <typename R, int L>
+__device__ __forceinline__ void col_issue_k(const FilmDev* __restrict__ films, const WorkItem* __restrict__ items,
+                                            int it, r4<R>* kst, uint64_t* bar) {
+    using C = ColCfg<R, L>;
+    const WorkItem w = items[it];
+    const FilmDev& F = films[w.film];
+    const int K1 = F.nx + 1, kx0 = w.blk * C::NC;
+    const int nv = min(C::NC, K1 - kx0);
+    const uint32_t bytes = (uint32_t)(sizeof(r4<R>) * (size_t)nv * (L + 1));
+    mbar_arrive_expect_tx(bar, bytes);
+    bulk_copy_g2s(kst, reinterpret_cast<const r4<R>*>(F.Khat) + (size_t)kx0 * (L + 1), bytes, bar);
+}
+
 template <typename R, int L>
 __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const FilmDev* __restrict__ films,
                                                                        const WorkItem* __restrict__ items, int nitems,
@@ -162,61 +254,105 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
     using C = ColCfg<R, L>;
     using FF = GroupFFT<R, L, false>;
     using FI = GroupFFT<R, L, true>;
-    constexpr int G = C::G, E = C::E, BUF = C::BUF;
+    constexpr int G = C::G, E = C::E, BUF = C::BUF, NC = C::NC;
+    constexpr int ny = L, L2 = 2 * L;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint64_t bars[2];   // 0: spectrum columns, 1: kernel columns
+    __shared__ int s_timeout;
     cx<R>* buf = reinterpret_cast<cx<R>*>(smem_raw);
-    cx<R>* twp = buf + C::NSIG * BUF;
-    cx<R>* pre = twp + TwTab<R, L>::size;
+    cx<R>* twp = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_TW);
+    cx<R>* pre = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_PRE);
+    cx<R>* xst = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_XST);
+    r4<R>* kst = reinterpret_cast<r4<R>*>(smem_raw + C::OFF_KST);
     const int tid = threadIdx.x, s = tid / G, t = tid % G;
     const int cl = s / 6, comp = (s % 6) >> 1, par = s & 1;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        s_timeout = 0;
+        mbar_init_fence();
+    }
+    __syncthreads();
+    const int it0 = blockIdx.x;
+    if (tid == 0 && col_item_has<R, L>(films, items, nitems, spec, it0)) {
+        col_issue_x<R, L>(films, items, it0, xst, &bars[0]);
+        col_issue_k<R, L>(films, items, it0, kst, &bars[1]);
+    }
+    uint32_t phase = 0;
     bool tables = false;
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    for (int it = it0; it < nitems; it += gridDim.x) {
+        const int nxt = it + gridDim.x;
+        const bool has = col_item_has<R, L>(films, items, nitems, spec, it);
+        const bool has_next = col_item_has<R, L>(films, items, nitems, spec, nxt);
+        if (!has) {   // nothing was fetched for this item (uniform over the block)
+            if (tid == 0 && has_next) {
+                fence_async_smem();
+                col_issue_x<R, L>(films, items, nxt, xst, &bars[0]);
+                col_issue_k<R, L>(films, items, nxt, kst, &bars[1]);
+            }
+            continue;
+        }
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
-        const StepState* st = F.st;
-        if (skip_item(spec, st)) continue;
-        if (!(spec.demag && F.demag_mat)) continue;
         if (!tables) {
             load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_col), TwTab<R, L>::size, pre,
                            reinterpret_cast<const cx<R>*>(F.tw_col), L);
             tables = true;
-            __syncthreads();
         }
-        const int nx = F.nx, K1 = nx + 1;
-        constexpr int ny = L;
-        const int kx = w.blk * C::NC + cl;
-        const bool valid = kx <= nx;
-        cx<R>* __restrict__ X = reinterpret_cast<cx<R>*>(F.X);
+        const bool okx = mbar_wait(&bars[0], phase);
+        const bool okk = mbar_wait(&bars[1], phase);
+        if (!(okx && okk)) s_timeout = 1;
+        phase ^= 1u;
+        __syncthreads();   // tables, staged columns, timeout flag
+        if (s_timeout) {
+            // a copy that never completed: report and leave without touching its buffers again
+            if (tid == 0) atomicExch(const_cast<int*>(&F.st->err_code), kErrAsyncTimeout);
+            return;
+        }
+        const bool run = !skip_item(spec, F.st);
+        const int K1 = F.nx + 1;
+        const int kx = w.blk * NC + cl;
+        const bool valid = kx < K1;
         cx<R> v[E];
+        if (run) {
 #pragma unroll
-        for (int r = 0; r < E; ++r) {
-            const int nn = t + G * r;
-            cx<R> x = valid ? X[(size_t)(comp * K1 + kx) * ny + nn] : mkc((R)0, (R)0);
-            v[r] = par ? cmul(x, pre[nn]) : x;
+            for (int r = 0; r < E; ++r) {
+                const int nn = t + G * r;
+                const cx<R> x = valid ? xst[((size_t)comp * NC + cl) * L + nn] : mkc((R)0, (R)0);
+                v[r] = par ? cmul(x, pre[nn]) : x;
+            }
         }
-        FF::run(v, t, buf + s * BUF, twp);
-        __syncthreads();
+        __syncthreads();   // staged spectrum consumed
+        if (tid == 0 && has_next) {
+            fence_async_smem();
+            col_issue_x<R, L>(films, items, nxt, xst, &bars[0]);
+        }
+        if (run) {
+            FF::run(v, t, buf + s * BUF, twp);
+            group_sync<G>();
 #pragma unroll
-        for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FF::out_index(t, i))] = v[i];
-        __syncthreads();
-        {
-            const r4<R>* __restrict__ Kp =
-                reinterpret_cast<const r4<R>*>(F.Kpar) + ((size_t)(valid ? kx : 0) * 2 + par) * ny;
+            for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FF::out_index(t, i))] = v[i];
+            __syncthreads();   // all components of the column transformed
+            const r4<R>* kc = kst + (size_t)cl * (L + 1);
             const cx<R>* sx = buf + (6 * cl + 0 + par) * BUF;
             const cx<R>* sy = buf + (6 * cl + 2 + par) * BUF;
             const cx<R>* sz = buf + (6 * cl + 4 + par) * BUF;
 #pragma unroll
             for (int r = 0; r < E; ++r) {
                 const int kk = t + G * r;
-                const r4<R> K = Kp[kk];
+                const int ky = 2 * kk + par;
+                // the kernel spectrum is even in ky except Kxy, which is odd
+                const bool up = ky > ny;
+                const r4<R> K = kc[up ? L2 - ky : ky];
+                const R kxy = up ? -K.y : K.y;
                 const int pi = padi<E>(kk);
                 cx<R> out;
                 if (comp == 0) {
                     const cx<R> Mx = sx[pi], My = sy[pi];
-                    out = mkc(K.x * Mx.re + K.y * My.re, K.x * Mx.im + K.y * My.im);
+                    out = mkc(K.x * Mx.re + kxy * My.re, K.x * Mx.im + kxy * My.im);
                 } else if (comp == 1) {
                     const cx<R> Mx = sx[pi], My = sy[pi];
-                    out = mkc(K.y * Mx.re + K.z * My.re, K.y * Mx.im + K.z * My.im);
+                    out = mkc(kxy * Mx.re + K.z * My.re, kxy * Mx.im + K.z * My.im);
                 } else {
                     const cx<R> Mz = sz[pi];
                     out = mkc(K.w * Mz.re, K.w * Mz.im);
@@ -224,29 +360,35 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
                 v[r] = out;
             }
         }
-        __syncthreads();
-        FI::run(v, t, buf + s * BUF, twp);
-        __syncthreads();
-        if (par) {
-#pragma unroll
-            for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FI::out_index(t, i))] = v[i];
+        __syncthreads();   // products formed: the signal buffers and staged kernel are free
+        if (tid == 0 && has_next) {
+            fence_async_smem();
+            col_issue_k<R, L>(films, items, nxt, kst, &bars[1]);
         }
-        __syncthreads();
-        if (!par && valid) {
-            const cx<R>* ob = buf + (s + 1) * BUF;
+        if (run) {
+            FI::run(v, t, buf + s * BUF, twp);
+            group_sync<G>();
+            if (par) {
 #pragma unroll
-            for (int i = 0; i < E; ++i) {
-                const int nn = FI::out_index(t, i);
-                X[(size_t)(comp * K1 + kx) * ny + nn] = v[i] + cmulc(ob[padi<E>(nn)], pre[nn]);
+                for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FI::out_index(t, i))] = v[i];
+            }
+            __syncthreads();   // odd-bin results visible to the even-bin groups
+            if (!par && valid) {
+                cx<R>* __restrict__ X = reinterpret_cast<cx<R>*>(F.X);
+                const cx<R>* ob = buf + (s + 1) * BUF;
+#pragma unroll
+                for (int i = 0; i < E; ++i) {
+                    const int nn = FI::out_index(t, i);
+                    X[((size_t)comp * K1 + kx) * ny + nn] = v[i] + cmulc(ob[padi<E>(nn)], pre[nn]);
+                }
             }
         }
-        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
 template <typename R, int L, bool LEAN>
-__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_inverse_fast(const FilmDev* __restrict__ films,
+__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((LEAN ? RowCfg<R, L>::MAXREG : RowCfg<R, L>::REGCAP)) k_row_inverse_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
                                                                             int nitems, EvalSpec spec) {
     using C = RowCfg<R, L>;
@@ -279,11 +421,17 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) k_row_inverse_fast(cons
             // stage this block's rows of the spectrum, [c][k][r], with contiguous
             // T-row chunks per (c, k) (the signal buffers are free here)
             cx<R>* stg = buf;
-            for (int e = tid; e < 3 * K1 * T; e += C::THREADS) {
-                const int r = e % T, ck = e / T;
-                const int j = j0 + r;
-                stg[e] = j < ny ? X[(size_t)ck * ny + j] : mkc((R)0, (R)0);
+            constexpr int PER = 16 / (int)sizeof(cx<R>);
+            for (int p = tid; p < 3 * K1 * T / PER; p += C::THREADS) {
+                const int e = p * PER, r = e % T, ck = e / T;
+                if (j0 + r < ny) {
+                    cp_async16(stg + e, X + (size_t)ck * ny + j0 + r);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < PER; ++q) stg[e + q] = mkc((R)0, (R)0);
+                }
             }
+            cp_async_wait_all();
             __syncthreads();
             auto xval = [&](int c, int k, int r) -> cx<R> {
                 if (k <= L) return stg[(c * K1 + k) * T + r];

@@ -215,10 +215,19 @@ __device__ __forceinline__ int pass_out_index(int t, int i) {
     return (b / NS) * NS * RADIX + (b % NS) + q * NS;
 }
 
+// Barrier over the threads of one transform group: a warp (or the part of one
+// holding whole groups) for G <= 32, the block otherwise.
+template <int G>
+__device__ __forceinline__ void group_sync() {
+    if constexpr (G <= 32) __syncwarp();
+    else __syncthreads();
+}
+
 // Full transform of one signal by its group.  On entry v[r] = x[t + G*r];
 // on exit v[i] = X[out_index(t, i)].  `buf` is this signal's padded exchange
-// buffer; `tw` the pass tables.  Every thread of the block must call this the
-// same number of times (it contains __syncthreads()).
+// buffer (only this group touches it inside); `tw` the pass tables.  Every
+// thread of the block must call this the same number of times (it contains
+// group_sync<G>(), a block barrier when G > 32).
 template <typename R, int L, bool INV>
 struct GroupFFT {
     using P = FPlan<R, L>;
@@ -235,13 +244,13 @@ struct GroupFFT {
         if constexpr (NP >= 2) {
 #pragma unroll
             for (int q = 0; q < E; ++q) buf[padi<E>(t * E + q)] = v[q];
-            __syncthreads();
+            group_sync<G>();
             group_pass<R, L, INV, P::RAD1, E>(v, t, buf, tw);
             if constexpr (NP >= 3) {
-                __syncthreads();
+                group_sync<G>();
 #pragma unroll
                 for (int i = 0; i < E; ++i) buf[padi<E>(pass_out_index<R, L, P::RAD1, E>(t, i))] = v[i];
-                __syncthreads();
+                group_sync<G>();
                 group_pass<R, L, INV, P::RAD2, E * P::RAD1>(v, t, buf, tw + TwTab<R, L>::size1);
             }
         }

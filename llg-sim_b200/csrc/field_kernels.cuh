@@ -22,6 +22,7 @@
 // and odd/odd for xy with zeros on the axes and Nyquist planes,
 // demag_fft_uniform.rs:1007-1071), so only its real part is stored, folded in ky.
 #pragma once
+#include "async_copy.cuh"
 #include "fft_smem.cuh"
 #include "types.cuh"
 
@@ -99,10 +100,12 @@ __device__ __forceinline__ void cp3(const R* a, R* o) {
 // (exchange.rs:45-222), anisotropy (anisotropy.rs:10-26), DMI (dmi.rs:67-209),
 // accumulated in that order.  With a geometry mask this is the _geom variant
 // (mod.rs:78-101).
-template <typename R>
-__device__ __forceinline__ void local_field(const FilmDev& F, const R* __restrict__ m, int i, int j, bool dmi_on,
-                                            const R* mc, R* b) {
-    const int nx = F.nx, ny = F.ny, n = nx * ny, idx = j * nx + i;
+// Neighbour values come from `nb(dir, out)`, dir 0..3 = (i-1, i+1, j-1, j+1);
+// it is called only for neighbours inside the film.
+template <typename R, typename NB>
+__device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i, int j, bool dmi_on, const R* mc,
+                                               R* b) {
+    const int nx = F.nx, ny = F.ny, idx = j * nx + i;
     b[0] = (R)0 + (R)F.bext[0];
     b[1] = (R)0 + (R)F.bext[1];
     b[2] = (R)0 + (R)F.bext[2];
@@ -115,19 +118,19 @@ __device__ __forceinline__ void local_field(const FilmDev& F, const R* __restric
         if (nx == 1) cp3(mc, mim);
         else if (i == 0) { if (he) ghost_x(mc, (R)-1, eta, dx, mim); else cp3(mc, mim); }
         else if (!cell_inside(F, idx - 1)) { if (he) ghost_x(mc, (R)-1, eta, dx, mim); else cp3(mc, mim); }
-        else ld3(m, n, idx - 1, mim);
+        else nb(0, mim);
         if (nx == 1) cp3(mc, mip);
         else if (i == nx - 1) { if (he) ghost_x(mc, (R)1, eta, dx, mip); else cp3(mc, mip); }
         else if (!cell_inside(F, idx + 1)) { if (he) ghost_x(mc, (R)1, eta, dx, mip); else cp3(mc, mip); }
-        else ld3(m, n, idx + 1, mip);
+        else nb(1, mip);
         if (ny == 1) cp3(mc, mjm);
         else if (j == 0) { if (he) ghost_y(mc, (R)-1, eta, dy, mjm); else cp3(mc, mjm); }
         else if (!cell_inside(F, idx - nx)) { if (he) ghost_y(mc, (R)-1, eta, dy, mjm); else cp3(mc, mjm); }
-        else ld3(m, n, idx - nx, mjm);
+        else nb(2, mjm);
         if (ny == 1) cp3(mc, mjp);
         else if (j == ny - 1) { if (he) ghost_y(mc, (R)1, eta, dy, mjp); else cp3(mc, mjp); }
         else if (!cell_inside(F, idx + nx)) { if (he) ghost_y(mc, (R)1, eta, dy, mjp); else cp3(mc, mjp); }
-        else ld3(m, n, idx + nx, mjp);
+        else nb(3, mjp);
         const R coeff = (R)F.exch;
         const R dx2 = dx * dx, dy2 = dy * dy;
 #pragma unroll
@@ -151,19 +154,19 @@ __device__ __forceinline__ void local_field(const FilmDev& F, const R* __restric
         if (nx == 1) { cp3(mc, mim); cp3(mc, mip); }
         else {
             if (i == 0) ghost_x(mc, (R)-1, eta, dx, mim);
-            else if (cell_inside(F, idx - 1)) ld3(m, n, idx - 1, mim);
+            else if (cell_inside(F, idx - 1)) nb(0, mim);
             else cp3(mc, mim);
             if (i == nx - 1) ghost_x(mc, (R)1, eta, dx, mip);
-            else if (cell_inside(F, idx + 1)) ld3(m, n, idx + 1, mip);
+            else if (cell_inside(F, idx + 1)) nb(1, mip);
             else cp3(mc, mip);
         }
         if (ny == 1) { cp3(mc, mjm); cp3(mc, mjp); }
         else {
             if (j == 0) ghost_y(mc, (R)-1, eta, dy, mjm);
-            else if (cell_inside(F, idx - nx)) ld3(m, n, idx - nx, mjm);
+            else if (cell_inside(F, idx - nx)) nb(2, mjm);
             else cp3(mc, mjm);
             if (j == ny - 1) ghost_y(mc, (R)1, eta, dy, mjp);
-            else if (cell_inside(F, idx + nx)) ld3(m, n, idx + nx, mjp);
+            else if (cell_inside(F, idx + nx)) nb(3, mjp);
             else cp3(mc, mjp);
         }
         const R pref = (R)F.dmi_pref;
@@ -175,6 +178,15 @@ __device__ __forceinline__ void local_field(const FilmDev& F, const R* __restric
         b[1] += pref * dmz_dy;
         b[2] += -pref * (dmx_dx + dmy_dy);
     }
+}
+
+template <typename R>
+__device__ __forceinline__ void local_field(const FilmDev& F, const R* __restrict__ m, int i, int j, bool dmi_on,
+                                            const R* mc, R* b) {
+    const int nx = F.nx, n = nx * F.ny, idx = j * nx + i;
+    local_field_nb<R>(
+        F, [&](int d, R* o) { ld3(m, n, d == 0 ? idx - 1 : d == 1 ? idx + 1 : d == 2 ? idx - nx : idx + nx, o); }, i, j,
+        dmi_on, mc, b);
 }
 
 // Energy density terms of one cell, FP64 (compute_energy_geom, energy.rs:131-275).
@@ -592,29 +604,59 @@ __device__ __forceinline__ void row_epilogue_lean(const FilmDev& F, const EvalSp
     const R pref = spec.rhs == RHS_LLG ? -gam / denom : -gam * alp / denom;
     const R c1 = spec.rhs == RHS_LLG ? (R)1 : (R)0;
     const R c2 = spec.rhs == RHS_LLG ? alp : (R)1;
-    for (int e = threadIdx.x; e < T * nx; e += blockDim.x) {
-        const int r = e / nx, i = e - r * nx, j = j0 + r;
+    const bool dmi_on = spec.dmi != 0;
+    // W consecutive cells per thread (nx is a multiple of W on this path): the
+    // centre, upper and lower rows as 16-byte vectors plus the two x halos, all
+    // loaded before any arithmetic
+    constexpr int W = Vec16<R>::W;
+    for (int e = threadIdx.x; e < T * nx / W; e += blockDim.x) {
+        const int c0 = e * W, r = c0 / nx, i0 = c0 - r * nx, j = j0 + r;
         if (j >= ny) continue;
-        const int idx = j * nx + i;
-        R mc[3];
-        ld3(msb, n, idx, mc);
-        R b[3];
-        local_field<R>(F, msb, i, j, spec.dmi != 0, mc, b);
-        if (do_fft) {
-            b[0] += dfield(r, i, 0);
-            b[1] += dfield(r, i, 1);
-            b[2] += dfield(r, i, 2);
+        const int idx0 = j * nx + i0;
+        Vec16<R> mc3[3], up3[3], dn3[3];
+        R hl[3] = {(R)0, (R)0, (R)0}, hr[3] = {(R)0, (R)0, (R)0};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            mc3[c] = ldv(msb + c * n + idx0);
+            up3[c] = j > 0 ? ldv(msb + c * n + idx0 - nx) : mc3[c];
+            dn3[c] = j + 1 < ny ? ldv(msb + c * n + idx0 + nx) : mc3[c];
+            if (i0 > 0) hl[c] = msb[c * n + idx0 - 1];
+            if (i0 + W < nx) hr[c] = msb[c * n + idx0 + W];
         }
-        // llg_rhs (llg.rs:20-32) / llg_rhs_relax (llg.rs:38-50)
-        const R t0 = mc[1] * b[2] - mc[2] * b[1];
-        const R t1 = mc[2] * b[0] - mc[0] * b[2];
-        const R t2 = mc[0] * b[1] - mc[1] * b[0];
-        const R u0 = mc[1] * t2 - mc[2] * t1;
-        const R u1 = mc[2] * t0 - mc[0] * t2;
-        const R u2 = mc[0] * t1 - mc[1] * t0;
-        kout[idx] = pref * (c1 * t0 + c2 * u0);
-        kout[n + idx] = pref * (c1 * t1 + c2 * u1);
-        kout[2 * n + idx] = pref * (c1 * t2 + c2 * u2);
+        Vec16<R> o3[3];
+#pragma unroll
+        for (int l = 0; l < W; ++l) {
+            const int i = i0 + l;
+            R mc[3] = {mc3[0].v[l], mc3[1].v[l], mc3[2].v[l]};
+            auto nb = [&](int d, R* o) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    if (d == 0) o[c] = l > 0 ? mc3[c].v[l > 0 ? l - 1 : 0] : hl[c];
+                    else if (d == 1) o[c] = l + 1 < W ? mc3[c].v[l + 1 < W ? l + 1 : 0] : hr[c];
+                    else if (d == 2) o[c] = up3[c].v[l];
+                    else o[c] = dn3[c].v[l];
+                }
+            };
+            R b[3];
+            local_field_nb<R>(F, nb, i, j, dmi_on, mc, b);
+            if (do_fft) {
+                b[0] += dfield(r, i, 0);
+                b[1] += dfield(r, i, 1);
+                b[2] += dfield(r, i, 2);
+            }
+            // llg_rhs (llg.rs:20-32) / llg_rhs_relax (llg.rs:38-50)
+            const R t0 = mc[1] * b[2] - mc[2] * b[1];
+            const R t1 = mc[2] * b[0] - mc[0] * b[2];
+            const R t2 = mc[0] * b[1] - mc[1] * b[0];
+            const R u0 = mc[1] * t2 - mc[2] * t1;
+            const R u1 = mc[2] * t0 - mc[0] * t2;
+            const R u2 = mc[0] * t1 - mc[1] * t0;
+            o3[0].v[l] = pref * (c1 * t0 + c2 * u0);
+            o3[1].v[l] = pref * (c1 * t1 + c2 * u1);
+            o3[2].v[l] = pref * (c1 * t2 + c2 * u2);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) stv(kout + c * n + idx0, o3[c]);
     }
 }
 

@@ -432,7 +432,6 @@ struct Engine final : EngineBase {
                         same = e;
                 if (same >= 0) {
                     F.Khat = fh[same].Khat;
-                    F.Kpar = fh[same].Kpar;
                     d_k64[f] = d_k64[same];
                 } else {
                     void* kh;
@@ -441,12 +440,6 @@ struct Engine final : EngineBase {
                     if ((rc = dalloc(&d_k64[f], sizeof(double) * 4 * (size_t)(nx + 1) * (ny + 1)))) return rc;
                     CUDA_TRY(build_demag_kernel(nx, ny, g[f].dx, g[f].dy, g[f].dz, sizeof(R) == 8, kh, d_k64[f],
                                                 stream));
-                    if (fast) {
-                        void* kp;
-                        if ((rc = dalloc(&kp, sizeof(r4<R>) * (size_t)(nx + 1) * 2 * ny))) return rc;
-                        CUDA_TRY(build_kernel_parity(nx, ny, sizeof(R) == 8, kh, kp, stream));
-                        F.Kpar = kp;
-                    }
                 }
             }
             for (int b = 0; b < F.nblk; ++b) rows.push_back(WorkItem{f, b});
@@ -477,17 +470,26 @@ struct Engine final : EngineBase {
         geom.col_threads = fast ? fc.col_threads : 256;
         CUDA_TRY(prepare_eval_kernels<R>(fast ? 0 : smem_row, fast ? 0 : smem_col));
         {
-            // persistent grids: one wave of resident blocks looping over the work items
-            int nsm = 148, rb = 1, cb = 1;
+            // persistent grids: at most one wave of resident blocks looping over the work
+            // items, shrunk to the fewest blocks that need the same number of rounds
+            int nsm = 148, fb = 1, ib = 1, ub = 1, cb = 1;
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
             if (fast) {
-                fast_occupancy<R>(nx0, ny0, &rb, &cb);
+                fast_occupancy<R>(nx0, ny0, &fb, &ib, &ub, &cb);
             } else {
-                rb = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_row, 1))));
+                fb = ib = ub = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_row, 1))));
                 cb = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_col, 1))));
             }
-            geom.grid_row = std::max(1, std::min(geom.n_row_items, nsm * rb));
-            geom.grid_col = std::max(1, std::min(std::max(geom.n_col_items, 1), nsm * cb));
+            auto balanced = [&](int items, int per_sm) {
+                items = std::max(items, 1);
+                const int slots = std::max(1, nsm * per_sm);
+                const int rounds = (items + slots - 1) / slots;
+                return (items + rounds - 1) / rounds;
+            };
+            geom.grid_row = balanced(geom.n_row_items, fb);
+            geom.grid_rinv = balanced(geom.n_row_items, ib);
+            geom.grid_rfull = balanced(geom.n_row_items, ub);
+            geom.grid_col = balanced(geom.n_col_items, cb);
         }
         if (any_demag && nf == 1) set_l2_window();
         CUDA_TRY(cudaStreamSynchronize(stream));
@@ -871,16 +873,31 @@ struct Engine final : EngineBase {
         std::unique_ptr<bool[]> inv(new bool[nf]);
         fsal_flags(kind, p, fmask, inv.get());
         if ((rc = set_control(c, p, inv.get(), false))) return rc;
+        // Poll the device every 32 attempts.  With a step-count target no film can
+        // finish in fewer attempts than its remaining steps, so a round launches at
+        // most the smallest remaining count (graphs of 8 attempts, then single ones)
+        // and no attempt is launched after every film is done.
         const int reps = 8;
-        cudaGraphExec_t ge = nullptr;
+        cudaGraphExec_t ge = nullptr, ge1 = nullptr;
         if ((rc = attempt_graph(kind, fmask, reps, &ge))) return rc;
         long long launched = 0;
         const long long limit = max_attempts > 0 ? max_attempts : (1LL << 40);
+        long long round = 32;
         for (;;) {
-            for (int q = 0; q < 4 && launched < limit; ++q) {
-                if ((rc = graph_launch(graph_key(kind, fmask, reps), ge))) return rc;
-                launched += reps;
+            if (n_acc > 0) {
+                round = 32;
+                for (int f = 0; f < nf; ++f)
+                    if (h_states[f].active) round = std::min(round, n_acc - (h_states[f].n_acc - acc0[f]));
+                round = std::max(round, 1LL);
             }
+            round = std::min(round, limit - launched);
+            long long q = 0;
+            for (; q + reps <= round; q += reps)
+                if ((rc = graph_launch(graph_key(kind, fmask, reps), ge))) return rc;
+            if (q < round && !ge1 && (rc = attempt_graph(kind, fmask, 1, &ge1))) return rc;
+            for (; q < round; ++q)
+                if ((rc = graph_launch(graph_key(kind, fmask, 1), ge1))) return rc;
+            launched += round;
             if ((rc = read_states())) return rc;
             bool any = false;
             for (int f = 0; f < nf; ++f) any |= h_states[f].active != 0;

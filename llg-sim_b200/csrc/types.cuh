@@ -86,7 +86,6 @@ struct FilmDev {
     void* bout;                   // field output (RHS_FIELD)
     void* X;                      // spectrum scratch
     const void* Khat;             // kernel spectrum
-    const void* Kpar;             // [nx+1][2][ny] real4: Khat at ky = 2k'+parity, unfolded, Kxy sign applied
     const uint8_t* mask;
     const void* tw_row;           // exp(-2 pi i k / (2nx)), k < 2nx
     const void* tw_col;           // exp(-2 pi i k / (2ny)), k < 2ny
