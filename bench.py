@@ -203,6 +203,71 @@ def params(L):
     return L.LLGParams(GAMMA, w["alpha"], w["dt0"], w["b_ext"])
 
 
+def batch_leg(L, torch, stream, world, max_over_ranks):
+    """Mixed-size batch: 256 films (nx 64..256, ny 32..128), FP32 RK45 for 1 ns each,
+    per-film dt, one engine: whole-batch cell-steps/s on the device clock."""
+    import workloads as W
+
+    films, run = W.mixed_film_batch(256)
+    b = L.Batch([f.grid(L) for f in films], [f.material(L) for f in films], L.FP32)
+    b.set_stream(stream.cuda_stream)
+    for i, f in enumerate(films):
+        b.set_state(i, L.init_uniform_with_noise(f.n, (1.0, 0.0, 0.0), run["noise"], 1000 + i))
+    ctl = (run["max_err"], run["headroom"], run["dt_min"], run["dt_max"])
+    P = [L.LLGParams(GAMMA, f.alpha, run["dt0"], f.b_ext) for f in films]
+    b.run_rk45(P, L.FULL, *ctl, n_accepted=3)   # graphs and kernels warm
+    for i, f in enumerate(films):
+        b.set_state(i, L.init_uniform_with_noise(f.n, (1.0, 0.0, 0.0), run["noise"], 1000 + i))
+    P = [L.LLGParams(GAMMA, f.alpha, run["dt0"], f.b_ext) for f in films]
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    acc, rej, t = b.run_rk45(P, L.FULL, *ctl, t_end=run["t_total"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    cells = np.array([f.n for f in films], dtype=np.float64)
+    b.close()
+    return {"workload": "256 films, nx in {64,96,128,192,256} x ny in {32,64,128}, 4x4x3 nm, Ms U[6e5,9e5], "
+                        "A U[1e-11,1.5e-11], alpha 0.02, 0-50 mT in-plane, FP32 RK45 max_err 1e-5, 1 ns each",
+            "value": float((cells * acc).sum()) * world / (ms * 1e-3), "unit": UNIT, "ms": ms,
+            "cells": int(cells.sum()), "accepted_mean": float(acc.mean()), "accepted_max": int(acc.max()),
+            "rejected": int(rej.sum()), "t_sim_min": float(t.min())}
+
+
+def flow_leg(L, torch, stream):
+    """128x32 film: relax (SP4 settings) then 1 ns at 20 mT in 10 ps windows, FP32 and FP64 wall times."""
+    import workloads as W
+
+    f, rx, run = W.film_128x32_relax_then_field()
+    out = {"workload": "128x32x1 film 4x4x3 nm, relax to max|m x B| 1e-4 T then 1 ns RK45 at 20 mT, <m> every "
+                       "10 ps"}
+    means = {}
+    for prec, name in ((L.FP64, "fp64"), (L.FP32, "fp32")):
+        sv = L.Solver(f.grid(L), f.material(L), prec)
+        sv.set_stream(stream.cuda_stream)
+        sv.set_state(f.m0)
+        t0 = time.perf_counter()
+        p = L.LLGParams(GAMMA, rx["alpha"], rx["dt0"], (0.0, 0.0, 0.0))
+        st = L.RelaxSettings.default(**{k: v for k, v in rx.items() if k not in ("alpha", "dt0")})
+        rep = sv.relax(p, L.FULL, st)
+        t1 = time.perf_counter()
+        p = L.LLGParams(GAMMA, run["alpha"], run["dt0"], f.b_ext)
+        acc = 0
+        for _ in range(int(round(run["t_total"] / run["dt_out"]))):
+            a, _, _ = sv.run_rk45(p, L.FULL, run["max_err"], run["headroom"], run["dt_min"], run["dt_max"],
+                                  t_end=run["dt_out"])
+            acc += a
+            sv.mean_m()
+        t2 = time.perf_counter()
+        means[name] = sv.mean_m()
+        out[name] = {"relax_s": t1 - t0, "relax_steps": int(rep.accepted_steps), "run_s": t2 - t1,
+                     "run_steps": int(acc), "mean_m": [float(x) for x in means[name]]}
+        sv.close()
+    out["mean_m_max_abs_diff"] = float(np.abs(means["fp32"] - means["fp64"]).max())
+    return out
+
+
 def run_gpu(args):
     import torch
 
@@ -333,7 +398,7 @@ def run_gpu(args):
     # FP32 vs FP64 at matched simulated time from the same initial state
     fp64 = None
     if not args.no_fp64:
-        k64 = max(1, min(args.steps, 60))
+        k64 = max(1, args.fp64_steps)
         a32 = make_solver(L, L.FP32)
         a64 = make_solver(L, L.FP64)
         for sv in (a32, a64):
@@ -359,6 +424,13 @@ def run_gpu(args):
         a32.close()
         a64.close()
 
+    batch = None
+    if not args.no_batch:
+        batch = batch_leg(L, torch, stream, world, max_over_ranks)
+    flow = None
+    if not args.no_flow:
+        flow = flow_leg(L, torch, stream)
+
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_budget)
@@ -373,7 +445,7 @@ def run_gpu(args):
                            "l2": "inputs larger than L2: ~190 MB per film working set (m, 7 torques, stage states, "
                                  "25 MB spectrum, 16 MB kernel) vs 126 MB L2"},
                 "clocks": clk, "gpu_launches": launches, "roofline": roofline, "roofline_step": roofline_step,
-                "e2e": e2e, "fp64": fp64, "cpu_baseline": cpu}
+                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     s.close()
     if dist is not None:
@@ -392,6 +464,9 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--fp64-steps", type=int, default=2000)
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-flow", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
