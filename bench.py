@@ -268,6 +268,65 @@ def flow_leg(L, torch, stream):
     return out
 
 
+def warmstart_leg(L, torch, stream, max_over_ranks, n_films=16, size=256):
+    """Holey films (0-6 holes, D U[0,2e-3], 0-30 mT), random m0, FP32 batched relax to
+    max |m x B| 1e-3 T: plain start vs the learned warm start (network on the tensor
+    cores, then relax).  Device-clock wall times of both arms; the final energies are
+    checked against the FP64 oracle evaluated on the GPU's final states."""
+    import workloads as W
+
+    wpath = os.path.join(ROOT, "llg-sim_b200", "weights", "warmstart_holey128.npy")
+    net = L.WarmStartNet(np.load(wpath))
+    films, rx = W.holey_film_batch(n_films, size, seed=77)
+    st = dict(torque_threshold=1e-3, max_err=rx["max_err"], headroom=rx["headroom"], dt_min=rx["dt_min"],
+              dt_max=rx["dt_max"], max_accepted_steps=60000)
+    out = {"workload": f"{n_films} films {size}x{size}, 4x4x3 nm, 0-6 holes r 8-24 cells, D U[0,2e-3], 0-30 mT "
+                       f"in-plane, random m0, FP32 relax to max|m x B| 1e-3 T (RK23, max 60000 steps)",
+           "weights": "llg-sim_b200/weights/warmstart_holey128.npy (trained on 1024 relaxed 128x128 films)"}
+    finals = {}
+    for arm in ("plain", "learned"):
+        b = L.Batch([f.grid(L) for f in films], [f.material(L) for f in films], L.FP32, masks=[f.mask for f in films])
+        b.set_stream(stream.cuda_stream)
+        for i, f in enumerate(films):
+            m = L.init_random(f.n, 900000 + i)
+            m[f.mask == 0] = 0.0
+            b.set_state(i, m)
+        P = [L.LLGParams(GAMMA, f.alpha, rx["dt0"], f.b_ext) for f in films]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if arm == "learned":
+            b.warm_start(net, [f.b_ext for f in films])
+        reps = b.relax(P, L.FULL, L.RelaxSettings.default(**st))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        en = [e.total() for e in b.compute_energy([f.b_ext for f in films])]
+        finals[arm] = ([b.get_state(i) for i in range(len(films))], en)
+        out[arm] = {"wall_s": ms * 1e-3, "steps_mean": float(np.mean([r.accepted_steps for r in reps])),
+                    "steps_max": int(max(r.accepted_steps for r in reps)),
+                    "converged": int(sum(r.stop_reason == 2 for r in reps)),
+                    "energy_mean_J": float(np.mean(en))}
+        b.close()
+    out["speedup"] = out["plain"]["wall_s"] / out["learned"]["wall_s"]
+    net.close()
+    try:
+        import oracle as O
+
+        worst = 0.0
+        for arm in ("plain", "learned"):
+            states, en = finals[arm]
+            for i, f in enumerate(films[:4]):
+                s = O.Solver(O.make_grid(f.nx, f.ny, f.dx, f.dy, f.dz),
+                             O.make_material(f.ms, f.a_ex, f.k_u, f.easy, f.dmi, f.demag), f.mask)
+                eo = s.energy(states[i], f.b_ext).total()
+                worst = max(worst, abs(en[i] - eo) / abs(eo))
+        out["energy_max_rel_diff_vs_fp64_oracle"] = worst
+    except Exception as exc:   # the oracle library is optional on a GPU box
+        out["energy_max_rel_diff_vs_fp64_oracle"] = f"unavailable: {exc}"
+    return out
+
+
 def run_gpu(args):
     import torch
 
@@ -430,6 +489,9 @@ def run_gpu(args):
     flow = None
     if not args.no_flow:
         flow = flow_leg(L, torch, stream)
+    warm = None
+    if not args.no_warmstart:
+        warm = warmstart_leg(L, torch, stream, max_over_ranks)
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -445,7 +507,7 @@ def run_gpu(args):
                            "l2": "inputs larger than L2: ~190 MB per film working set (m, 7 torques, stage states, "
                                  "25 MB spectrum, 16 MB kernel) vs 126 MB L2"},
                 "clocks": clk, "gpu_launches": launches, "roofline": roofline, "roofline_step": roofline_step,
-                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "cpu_baseline": cpu}
+                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "warm_start": warm, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     s.close()
     if dist is not None:
@@ -467,6 +529,7 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2000)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-flow", action="store_true")
+    ap.add_argument("--no-warmstart", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -247,6 +247,24 @@ void llg_init_random(int64_t n, uint64_t seed, double* m_aos);                  
 void llg_init_uniform_with_noise(int64_t n, const double dir[3], double noise,  /* :43-56 */
                                  uint64_t seed, double* m_aos);
 
+/* ---------------------------------------------------------------------------
+ * Learned warm start.  No reference counterpart: a six-layer 3x3 convolutional
+ * network (32 channels, BF16 weights and activations, FP32 accumulation on the
+ * tensor cores) maps (m, inside, B_ext / 0.05 T) to a proposal m that a relax can
+ * start from.  Parameters are FP32, per layer W[cout][3][3][cin] then b[cout],
+ * with (cin, cout) = (7,32), (32,32) x4, (32,3); llg_warmstart_param_count()
+ * gives the total.
+ * ------------------------------------------------------------------------- */
+typedef struct llg_warmstart llg_warmstart;
+int64_t llg_warmstart_param_count(void);
+int llg_warmstart_create(llg_ctx* ctx, const float* params, int64_t n_params, llg_warmstart** out);
+int llg_warmstart_destroy(llg_warmstart* w);
+/* host buffers: m_aos [nimg][ny*nx][3], mask [nimg][ny*nx] or NULL, b_ext [nimg][3] -> out_aos */
+int llg_warmstart_forward(llg_warmstart* w, int64_t nimg, int64_t ny, int64_t nx, const double* m_aos,
+                          const uint8_t* mask, const double* b_ext, double* out_aos);
+/* replace every film's state by the proposal computed from it on the device; b_ext [n][3] */
+int llg_batch_warm_start(llg_batch* b, llg_warmstart* w, const double* b_ext);
+
 #ifdef __cplusplus
 }
 #endif

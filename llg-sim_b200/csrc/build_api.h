@@ -67,4 +67,16 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col);
 template <typename R>
 cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s);
 
+// Learned warm-start network (conv_tc.cu).
+namespace ws {
+struct Net;
+long long net_param_count();
+cudaError_t net_create(const float* params, long long n, int device, Net** out);
+void net_destroy(Net* net);
+int net_error();
+template <typename R>
+cudaError_t net_apply(Net* net, const R* m_in, R* m_out, const uint8_t* mask, const double* bext_host, int nimg,
+                      int ny, int nx, cudaStream_t s);
+}  // namespace ws
+
 }  // namespace llg

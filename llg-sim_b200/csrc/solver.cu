@@ -242,6 +242,7 @@ struct EngineBase {
     virtual int kernel_kspace(int f, double* out) = 0;
     virtual int profile_stage(const llg_params* p, int fmask, int reps, double* ms3) = 0;
     virtual long long launch_count() = 0;
+    virtual int warm_start(ws::Net* net, const double* bext3n) = 0;
 };
 
 // LLG_B200_GENERIC_FFT=1 selects the generic shared-memory Stockham kernels
@@ -595,6 +596,24 @@ struct Engine final : EngineBase {
         for (int e = 0; e < nf; ++e) iv[e] = e == f;
         if ((rc = set_control(idle_control(), nullptr, iv.get(), true))) return rc;
         CUDA_TRY(cudaStreamSynchronize(stream));
+        return LLG_OK;
+    }
+
+    // Replace every film's state by the warm-start network's proposal, on the device.
+    int warm_start(ws::Net* net, const double* bext3n) override {
+        int rc;
+        if ((rc = read_states())) return rc;
+        for (int f = 0; f < nf; ++f) {
+            R* m = reinterpret_cast<R*>(const_cast<void*>(fh[f].m[h_states[f].cur ? 1 : 0]));
+            CUDA_TRY(ws::net_apply<R>(net, m, m, fh[f].has_mask ? fh[f].mask : nullptr, bext3n + 3 * f, 1,
+                                      fh[f].ny, fh[f].nx, stream));
+        }
+        invalidate_fsal_host();
+        std::unique_ptr<bool[]> iv(new bool[nf]);
+        for (int e = 0; e < nf; ++e) iv[e] = true;
+        if ((rc = set_control(idle_control(), nullptr, iv.get(), true))) return rc;
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        if (ws::net_error()) return set_error(LLG_ERR_TIMEOUT, "warm-start network: tensor-core wait timed out");
         return LLG_OK;
     }
 
@@ -1193,6 +1212,11 @@ using llg::set_error;
 // Lets other translation units report through llg_last_error().
 void llg_set_error_message(const char* msg) { llg::g_last_error = msg ? msg : ""; }
 
+struct llg_warmstart {
+    llg::ws::Net* net;
+    int device;
+};
+
 namespace {
 int check_device(int device) {
     int count = 0;
@@ -1458,6 +1482,72 @@ int llg_batch_launch_count(llg_batch* b, int64_t* out) {
     if (rc) return rc;
     *out = b->eng->launch_count();
     return LLG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Learned warm start (no reference counterpart)
+// ---------------------------------------------------------------------------
+int64_t llg_warmstart_param_count(void) { return llg::ws::net_param_count(); }
+
+int llg_warmstart_create(llg_ctx* ctx, const float* params, int64_t n_params, llg_warmstart** out) {
+    if (!ctx || !params || !out) return set_error(LLG_ERR_INVALID, "null argument");
+    if (n_params != llg::ws::net_param_count())
+        return set_error(LLG_ERR_INVALID, "expected %lld parameters, got %lld",
+                         (long long)llg::ws::net_param_count(), (long long)n_params);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return set_error(LLG_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    llg::ws::Net* net = nullptr;
+    e = llg::ws::net_create(params, n_params, ctx->device, &net);
+    if (e != cudaSuccess) return set_error(LLG_ERR_CUDA, "warm-start network: %s", cudaGetErrorString(e));
+    *out = new llg_warmstart{net, ctx->device};
+    return LLG_OK;
+}
+
+int llg_warmstart_destroy(llg_warmstart* w) {
+    if (!w) return LLG_OK;
+    cudaSetDevice(w->device);
+    llg::ws::net_destroy(w->net);
+    delete w;
+    return LLG_OK;
+}
+
+int llg_warmstart_forward(llg_warmstart* w, int64_t nimg, int64_t ny, int64_t nx, const double* m_aos,
+                          const uint8_t* mask, const double* b_ext, double* out_aos) {
+    if (!w || !m_aos || !b_ext || !out_aos) return set_error(LLG_ERR_INVALID, "null argument");
+    if (nimg < 1 || ny < 1 || nx < 1 || nimg * ny * nx > (1LL << 28))
+        return set_error(LLG_ERR_INVALID, "bad sizes %lld x %lld x %lld", (long long)nimg, (long long)ny,
+                         (long long)nx);
+    cudaError_t e = cudaSetDevice(w->device);
+    if (e != cudaSuccess) return set_error(LLG_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    const long long hw = ny * nx, cells = nimg * hw;
+    std::vector<float> soa((size_t)cells * 3);
+    for (long long im = 0; im < nimg; ++im)
+        for (long long c = 0; c < hw; ++c)
+            for (int q = 0; q < 3; ++q) soa[(size_t)im * 3 * hw + q * hw + c] = (float)m_aos[3 * (im * hw + c) + q];
+    float* d_m = nullptr;
+    uint8_t* d_mask = nullptr;
+    e = cudaMalloc(&d_m, sizeof(float) * soa.size());
+    if (e == cudaSuccess && mask) e = cudaMalloc(&d_mask, (size_t)cells);
+    if (e == cudaSuccess) e = cudaMemcpy(d_m, soa.data(), sizeof(float) * soa.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && mask) e = cudaMemcpy(d_mask, mask, (size_t)cells, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = llg::ws::net_apply<float>(w->net, d_m, d_m, d_mask, b_ext, (int)nimg, (int)ny, (int)nx, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(soa.data(), d_m, sizeof(float) * soa.size(), cudaMemcpyDeviceToHost);
+    cudaFree(d_m);
+    cudaFree(d_mask);
+    if (e != cudaSuccess) return set_error(LLG_ERR_CUDA, "warm-start forward: %s", cudaGetErrorString(e));
+    if (llg::ws::net_error()) return set_error(LLG_ERR_TIMEOUT, "warm-start network: tensor-core wait timed out");
+    for (long long im = 0; im < nimg; ++im)
+        for (long long c = 0; c < hw; ++c)
+            for (int q = 0; q < 3; ++q) out_aos[3 * (im * hw + c) + q] = soa[(size_t)im * 3 * hw + q * hw + c];
+    return LLG_OK;
+}
+
+int llg_batch_warm_start(llg_batch* b, llg_warmstart* w, const double* b_ext) {
+    int rc = bind(b);
+    if (!rc && (!w || !b_ext)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    if (!rc && w->device != b->device) rc = set_error(LLG_ERR_INVALID, "network and batch on different devices");
+    return rc ? rc : b->eng->warm_start(w->net, b_ext);
 }
 
 // XorShift64 seeded initial states (initial_states.rs:43-68, 230-254).

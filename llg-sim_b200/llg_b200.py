@@ -149,6 +149,11 @@ def lib():
             "llg_batch_relax": (C.c_int, [vp, P(_Params), i32, P(RelaxSettings), P(RelaxReport)]),
             "llg_batch_compute_energy": (C.c_int, [vp, dp, P(EnergyBreakdown)]),
             "llg_batch_launch_count": (C.c_int, [vp, P(i64)]),
+            "llg_warmstart_param_count": (i64, []),
+            "llg_warmstart_create": (C.c_int, [vp, P(C.c_float), i64, P(vp)]),
+            "llg_warmstart_destroy": (C.c_int, [vp]),
+            "llg_warmstart_forward": (C.c_int, [vp, i64, i64, i64, dp, vp, dp, dp]),
+            "llg_batch_warm_start": (C.c_int, [vp, vp, dp]),
             "llg_init_random": (None, [i64, C.c_uint64, dp]),
             "llg_init_uniform_with_noise": (None, [i64, dp, C.c_double, C.c_uint64, dp]),
         }
@@ -453,6 +458,11 @@ class Batch:
             p.dt = P[i].dt
         return list(reps)
 
+    def warm_start(self, net, b_exts):
+        """Replace every film's state by the warm-start network's proposal (on the device)."""
+        be = np.ascontiguousarray(np.asarray(b_exts, dtype=np.float64).reshape(self.n, 3))
+        _check(lib().llg_batch_warm_start(self.h, net.h, _dp(be)))
+
     def compute_energy(self, b_exts):
         be = np.ascontiguousarray(np.asarray(b_exts, dtype=np.float64).reshape(self.n, 3))
         out = (EnergyBreakdown * self.n)()
@@ -470,6 +480,49 @@ def demag_field_noalloc(nx, ny, ms, m_dev_ptr, kernel_planes_dev_ptr, b_dev_ptr,
     _check(lib().llg_demag_field_noalloc(int(nx), int(ny), float(ms), C.c_void_p(m_dev_ptr),
                                          C.c_void_p(kernel_planes_dev_ptr), C.c_void_p(b_dev_ptr),
                                          C.c_void_p(stream_ptr)))
+
+
+class WarmStartNet:
+    """Learned warm start: six 3x3 convolutions (32 channels, BF16 on the tensor
+    cores) from (m, inside, B_ext/0.05 T) to a proposal m.  `params` is the flat
+    FP32 vector of per-layer W[cout][3][3][cin] then b[cout]."""
+
+    LAYERS = ((7, 32), (32, 32), (32, 32), (32, 32), (32, 32), (32, 3))
+
+    @staticmethod
+    def param_count():
+        return int(lib().llg_warmstart_param_count())
+
+    def __init__(self, params, device=0):
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float32).reshape(-1))
+        h = C.c_void_p()
+        _check(lib().llg_warmstart_create(_ctx(device), p.ctypes.data_as(C.POINTER(C.c_float)), p.size,
+                                          C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().llg_warmstart_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, m, mask, b_ext, ny, nx):
+        """m [nimg, ny*nx, 3] (or one image), mask [nimg, ny*nx] or None, b_ext [nimg, 3]."""
+        m = np.ascontiguousarray(np.asarray(m, dtype=np.float64))
+        nimg = m.size // (3 * ny * nx)
+        out = np.empty_like(m)
+        be = np.ascontiguousarray(np.asarray(b_ext, dtype=np.float64).reshape(nimg, 3))
+        mp = None
+        if mask is not None:
+            mk = np.ascontiguousarray(np.asarray(mask).reshape(-1).astype(np.uint8))
+            mp = mk.ctypes.data_as(C.c_void_p)
+        _check(lib().llg_warmstart_forward(self.h, nimg, int(ny), int(nx), _dp(m), mp, _dp(be), _dp(out)))
+        return out
 
 
 def init_random(n, seed):

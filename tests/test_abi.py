@@ -40,3 +40,9 @@ def test_default_relax_settings_match_oracle(gpu, orc):
     b = orc.default_relax_settings()
     for name, _ in gpu.RelaxSettings._fields_:
         assert getattr(a, name) == getattr(b, name), name
+
+
+def test_warmstart_param_count_matches_reference_layout(gpu):
+    import warmstart_ref
+
+    assert gpu.WarmStartNet.param_count() == warmstart_ref.param_count() == 39907
