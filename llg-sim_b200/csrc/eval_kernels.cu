@@ -101,6 +101,12 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
         if (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
             cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ColCfg<R, L>::SMEM);
+        // the whole unified L1/shared array as shared memory, so that occupancy is
+        // bounded by registers and the blocks' own shared memory only
+        cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_row_inverse_fast<R, L, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_row_inverse_fast<R, L, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     };
     for (int L : {16, 32, 64, 128, 256, 512, 1024, 2048}) dispatch_L<R>(L, set_all);
     return cudaGetLastError();

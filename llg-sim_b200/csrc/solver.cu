@@ -287,6 +287,7 @@ struct Engine final : EngineBase {
     bool l2_window = false;
     cudaStreamAttrValue l2_attr{};
     RelaxSettingsDev relax_graph_settings{};
+    int fb_occ = 1, ib_occ = 1, ub_occ = 1, cb_occ = 1;   // resident blocks per SM of the fast passes
 
     int nfilms() const override { return nf; }
     int64_t cells(int f) const override { return grids[f].nx * grids[f].ny; }
@@ -491,9 +492,82 @@ struct Engine final : EngineBase {
             geom.grid_rinv = balanced(geom.n_row_items, ib);
             geom.grid_rfull = balanced(geom.n_row_items, ub);
             geom.grid_col = balanced(geom.n_col_items, cb);
+            fb_occ = fb;
+            ib_occ = ib;
+            ub_occ = ub;
+            cb_occ = cb;
         }
         if (any_demag && nf == 1) set_l2_window();
+        if (fast && (rc = autotune_grids(nsm_count(), fb_occ, ib_occ, ub_occ, cb_occ))) return rc;
         CUDA_TRY(cudaStreamSynchronize(stream));
+        return LLG_OK;
+    }
+
+    int nsm_count() const {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+        return nsm;
+    }
+
+    // Grid autotuner of the register-FFT passes: for each pass, time the candidate
+    // persistent grid sizes (for 1..occupancy resident blocks per SM: the fewest
+    // blocks that need the same number of rounds over the work items, and the full
+    // resident wave) on a representative RK45 stage and keep the fastest.  Runs once
+    // per engine, on the engine's own buffers, before any state is set.
+    int autotune_grids(int nsm, int fb, int ib, int ub, int cb) {
+        if (const char* e = std::getenv("LLG_B200_NO_AUTOTUNE"))
+            if (e[0] == '1') return LLG_OK;
+        int rc;
+        if ((rc = set_control(idle_control(), nullptr, nullptr, true))) return rc;
+        EvalSpec stage = base_spec(LLG_FIELD_FULL);
+        stage.rhs = RHS_LLG;
+        combo(stage, MB_S0, {KB_K1, KB_K2, KB_K3}, {dp5::A41, dp5::A42, dp5::A43});
+        stage.k_out = KB_K4;
+        EvalSpec full = stage;
+        full.reduce = 1;
+        cudaEvent_t e0, e1;
+        CUDA_TRY(cudaEventCreate(&e0));
+        CUDA_TRY(cudaEventCreate(&e1));
+        auto candidates = [&](int items, int occ) {
+            std::vector<int> c;
+            items = std::max(items, 1);
+            for (int per = 1; per <= occ; ++per) {
+                const int slots = std::max(1, nsm * per), rounds = (items + slots - 1) / slots;
+                c.push_back((items + rounds - 1) / rounds);
+                c.push_back(std::min(items, slots));
+            }
+            std::sort(c.begin(), c.end());
+            c.erase(std::unique(c.begin(), c.end()), c.end());
+            return c;
+        };
+        auto tune = [&](int which, const EvalSpec& spec, int* grid, int items, int occ) -> int {
+            float best = 1e30f;
+            int best_g = *grid;
+            for (int g : candidates(items, occ)) {
+                *grid = g;
+                for (int w = 0; w < 2; ++w) CUDA_TRY(launch_one<R>(which, spec, geom, stream));
+                CUDA_TRY(cudaEventRecord(e0, stream));
+                for (int r = 0; r < 4; ++r) CUDA_TRY(launch_one<R>(which, spec, geom, stream));
+                CUDA_TRY(cudaEventRecord(e1, stream));
+                CUDA_TRY(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) {
+                    best = ms;
+                    best_g = g;
+                }
+            }
+            *grid = best_g;
+            return LLG_OK;
+        };
+        const int nr = geom.n_row_items, nc = geom.n_col_items;
+        if ((rc = tune(0, stage, &geom.grid_row, nr, fb))) return rc;
+        if (any_demag && (rc = tune(1, stage, &geom.grid_col, nc, cb))) return rc;
+        if ((rc = tune(2, stage, &geom.grid_rinv, nr, ib))) return rc;
+        if ((rc = tune(2, full, &geom.grid_rfull, nr, ub))) return rc;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        invalidate_fsal_host();
         return LLG_OK;
     }
 
