@@ -46,6 +46,7 @@ struct LaunchGeom {
 // block, threads and shared memory; ok = false when the size has no fast path.
 struct FastCfg {
     bool ok;
+    bool ok_row, ok_col;   // a register-FFT row / column kernel exists for this nx / ny
     int T, NC, row_threads, col_threads;
     size_t smem_row, smem_col;
     int twp_row_size, twp_col_size;

@@ -53,7 +53,9 @@ FastCfg fast_config(int nx, int ny) {
         c.smem_col = ColCfg<R, L>::SMEM;
         c.twp_col_size = TwTab<R, L>::size;
     });
-    c.ok = okr && okc && c.smem_row <= kSmemMax && c.smem_col + kStaticSmemCol <= kSmemMax;
+    c.ok_row = okr && c.smem_row <= kSmemMax;
+    c.ok_col = okc && c.smem_col + kStaticSmemCol <= kSmemMax;
+    c.ok = c.ok_row && c.ok_col;
     return c;
 }
 

@@ -9,6 +9,7 @@
 // a CUDA graph and replayed without host round trips; films advance with their
 // own dt and acceptance.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -287,7 +288,11 @@ struct Engine final : EngineBase {
     bool l2_window = false;
     cudaStreamAttrValue l2_attr{};
     RelaxSettingsDev relax_graph_settings{};
-    int fb_occ = 1, ib_occ = 1, ub_occ = 1, cb_occ = 1;   // resident blocks per SM of the fast passes
+    // launch segments: films grouped by the row (rseg) / column (cseg) kernel they use,
+    // with the resident blocks per SM of each segment's kernels
+    std::vector<LaunchGeom> rseg, cseg;
+    std::vector<std::array<int, 3>> rocc;
+    std::vector<int> cocc;
 
     int nfilms() const override { return nf; }
     int64_t cells(int f) const override { return grids[f].nx * grids[f].ny; }
@@ -313,9 +318,13 @@ struct Engine final : EngineBase {
         return LLG_OK;
     }
 
+    // One evaluation: row forward, column (with demag), row inverse, one launch per segment.
     int eval(const EvalSpec& e) {
-        CUDA_TRY(launch_eval<R>(e, geom, stream));
-        launches += (e.demag && geom.any_demag) ? 3 : 2;
+        for (auto& sg : rseg) CUDA_TRY(launch_one<R>(0, e, sg, stream));
+        if (e.demag && geom.any_demag)
+            for (auto& sg : cseg) CUDA_TRY(launch_one<R>(1, e, sg, stream));
+        for (auto& sg : rseg) CUDA_TRY(launch_one<R>(2, e, sg, stream));
+        launches += 2 * (long long)rseg.size() + ((e.demag && geom.any_demag) ? (long long)cseg.size() : 0);
         return LLG_OK;
     }
 
@@ -333,33 +342,38 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaMallocHost(&h_states, sizeof(StepState) * nf));
         CUDA_TRY(cudaMallocHost(&h_relax, sizeof(RelaxStateDev) * nf));
         CUDA_TRY(cudaMallocHost(&h_ctl, sizeof(FilmCtl) * nf));
-        // kernel choice: register-FFT kernels when every film shares one power-of-two shape
-        bool same_shape = true;
-        for (int f = 1; f < nf; ++f) same_shape &= g[f].nx == g[0].nx && g[f].ny == g[0].ny;
+        // kernel choice per film and pass: register-FFT row kernels where nx has one,
+        // register-FFT column kernel where ny has one; the generic kernels otherwise.
+        // Films are grouped into launch segments by that choice (one launch per segment
+        // and pass), so a mixed batch still runs its power-of-two films on the fast path.
         for (int f = 0; f < nf; ++f) any_demag |= m[f].demag != 0;
-        const int nx0 = (int)g[0].nx, ny0 = (int)g[0].ny;
-        const FastCfg fc = fast_config<R>(nx0, ny0);
-        const bool fast = same_shape && fc.ok && !force_generic();
-        const int T = fast ? fc.T : 2;
-        const int NC = fast ? fc.NC : 1;
-        const int G = T + (T + 1) / 2;
-        size_t smem_row = 0, smem_col = 0;
+        const bool gen = force_generic();
+        std::vector<FastCfg> fcs(nf);
+        std::vector<char> frow(nf), fcol(nf);
+        for (int f = 0; f < nf; ++f) {
+            fcs[f] = fast_config<R>((int)g[f].nx, (int)g[f].ny);
+            frow[f] = !gen && fcs[f].ok_row;
+            fcol[f] = !gen && fcs[f].ok_col;
+        }
+        size_t smem_row = 0, smem_col = 0;   // generic kernels
         for (int f = 0; f < nf; ++f) {
             if (!m[f].demag) continue;
-            smem_row = std::max(smem_row, 4 * (size_t)G * g[f].nx * sizeof(cx<R>));
-            smem_col = std::max(smem_col, 12 * (size_t)g[f].ny * sizeof(cx<R>));
+            if (!frow[f]) smem_row = std::max(smem_row, 4 * (size_t)3 * g[f].nx * sizeof(cx<R>));
+            if (!fcol[f]) smem_col = std::max(smem_col, 12 * (size_t)g[f].ny * sizeof(cx<R>));
         }
         const size_t smem_max = 227 * 1024;
-        if (!fast && (smem_row > smem_max || smem_col > smem_max))
+        if (smem_row > smem_max || smem_col > smem_max)
             return set_error(LLG_ERR_INVALID, "a film exceeds the in-shared-memory FFT limit for this precision");
         int rc;
         if ((rc = dalloc(&d_states, sizeof(StepState) * nf))) return rc;
         CUDA_TRY(cudaMemsetAsync(d_states, 0, sizeof(StepState) * nf, stream));
         if ((rc = dalloc(&d_relax, sizeof(RelaxStateDev) * nf))) return rc;
         if ((rc = dalloc(&d_ctl, sizeof(FilmCtl) * nf))) return rc;
-        std::vector<WorkItem> rows, cols;
+        std::map<int, std::vector<WorkItem>> rows_by, cols_by;   // segment key: L of the fast kernel, 0 generic
         for (int f = 0; f < nf; ++f) {
             const int nx = (int)g[f].nx, ny = (int)g[f].ny;
+            const int T = frow[f] ? fcs[f].T : 2;
+            const int NC = fcol[f] ? fcs[f].NC : 1;
             const int64_t n = (int64_t)nx * ny;
             max_cells = std::max(max_cells, n);
             const size_t plane = sizeof(R) * 3 * (size_t)n;
@@ -416,7 +430,8 @@ struct Engine final : EngineBase {
                 CUDA_TRY(launch_twiddles(tw_col, 2 * ny, sizeof(R) == 8, stream));
                 F.tw_row = tw_row;
                 F.tw_col = tw_col;
-                if (fast) {
+                if (frow[f] || fcol[f]) {
+                    const FastCfg& fc = fcs[f];
                     void* twp_row;
                     void* twp_col;
                     if ((rc = dalloc(&twp_row, sizeof(cx<R>) * (size_t)std::max(fc.twp_row_size, 1)))) return rc;
@@ -444,10 +459,20 @@ struct Engine final : EngineBase {
                                                 stream));
                 }
             }
-            for (int b = 0; b < F.nblk; ++b) rows.push_back(WorkItem{f, b});
+            for (int b = 0; b < F.nblk; ++b) rows_by[frow[f] ? nx : 0].push_back(WorkItem{f, b});
             const int ncb = (nx + 1 + NC - 1) / NC;
             if (m[f].demag)
-                for (int b = 0; b < ncb; ++b) cols.push_back(WorkItem{f, b});
+                for (int b = 0; b < ncb; ++b) cols_by[fcol[f] ? ny : 0].push_back(WorkItem{f, b});
+        }
+        std::vector<WorkItem> rows, cols;
+        std::vector<std::pair<int, std::pair<size_t, size_t>>> rspan, cspan;   // key, [offset, count)
+        for (auto& kv : rows_by) {
+            rspan.push_back({kv.first, {rows.size(), kv.second.size()}});
+            rows.insert(rows.end(), kv.second.begin(), kv.second.end());
+        }
+        for (auto& kv : cols_by) {
+            cspan.push_back({kv.first, {cols.size(), kv.second.size()}});
+            cols.insert(cols.end(), kv.second.begin(), kv.second.end());
         }
         if ((rc = dalloc(&d_films, sizeof(FilmDev) * nf))) return rc;
         CUDA_TRY(cudaMemcpyAsync(d_films, fh.data(), sizeof(FilmDev) * nf, cudaMemcpyHostToDevice, stream));
@@ -466,39 +491,48 @@ struct Engine final : EngineBase {
         geom.smem_row = smem_row;
         geom.smem_col = smem_col;
         geom.any_demag = any_demag;
-        geom.fast_row = fast ? nx0 : 0;
-        geom.fast_col = fast ? ny0 : 0;
-        geom.row_threads = fast ? fc.row_threads : 256;
-        geom.col_threads = fast ? fc.col_threads : 256;
-        CUDA_TRY(prepare_eval_kernels<R>(fast ? 0 : smem_row, fast ? 0 : smem_col));
+        geom.fast_row = 0;
+        geom.fast_col = 0;
+        CUDA_TRY(prepare_eval_kernels<R>(smem_row, smem_col));
         {
             // persistent grids: at most one wave of resident blocks looping over the work
             // items, shrunk to the fewest blocks that need the same number of rounds
-            int nsm = 148, fb = 1, ib = 1, ub = 1, cb = 1;
-            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            if (fast) {
-                fast_occupancy<R>(nx0, ny0, &fb, &ib, &ub, &cb);
-            } else {
-                fb = ib = ub = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_row, 1))));
-                cb = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_col, 1))));
-            }
+            const int nsm = nsm_count();
             auto balanced = [&](int items, int per_sm) {
                 items = std::max(items, 1);
                 const int slots = std::max(1, nsm * per_sm);
                 const int rounds = (items + slots - 1) / slots;
                 return (items + rounds - 1) / rounds;
             };
-            geom.grid_row = balanced(geom.n_row_items, fb);
-            geom.grid_rinv = balanced(geom.n_row_items, ib);
-            geom.grid_rfull = balanced(geom.n_row_items, ub);
-            geom.grid_col = balanced(geom.n_col_items, cb);
-            fb_occ = fb;
-            ib_occ = ib;
-            ub_occ = ub;
-            cb_occ = cb;
+            const int gen_r = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_row, 1))));
+            const int gen_c = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_col, 1))));
+            for (auto& sp : rspan) {
+                LaunchGeom s = geom;
+                s.row_items = d_row_items + sp.second.first;
+                s.n_row_items = (int)sp.second.second;
+                s.fast_row = sp.first;
+                int fb = gen_r, ib = gen_r, ub = gen_r, cb = 1;
+                if (sp.first) fast_occupancy<R>(sp.first, 0, &fb, &ib, &ub, &cb);
+                s.grid_row = balanced(s.n_row_items, fb);
+                s.grid_rinv = balanced(s.n_row_items, ib);
+                s.grid_rfull = balanced(s.n_row_items, ub);
+                rseg.push_back(s);
+                rocc.push_back({fb, ib, ub});
+            }
+            for (auto& sp : cspan) {
+                LaunchGeom s = geom;
+                s.col_items = d_col_items + sp.second.first;
+                s.n_col_items = (int)sp.second.second;
+                s.fast_col = sp.first;
+                int fb = 1, ib = 1, ub = 1, cb = gen_c;
+                if (sp.first) fast_occupancy<R>(0, sp.first, &fb, &ib, &ub, &cb);
+                s.grid_col = balanced(s.n_col_items, cb);
+                cseg.push_back(s);
+                cocc.push_back(cb);
+            }
         }
         if (any_demag && nf == 1) set_l2_window();
-        if (fast && (rc = autotune_grids(nsm_count(), fb_occ, ib_occ, ub_occ, cb_occ))) return rc;
+        if ((rc = autotune_grids(nsm_count()))) return rc;
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
     }
@@ -514,7 +548,7 @@ struct Engine final : EngineBase {
     // blocks that need the same number of rounds over the work items, and the full
     // resident wave) on a representative RK45 stage and keep the fastest.  Runs once
     // per engine, on the engine's own buffers, before any state is set.
-    int autotune_grids(int nsm, int fb, int ib, int ub, int cb) {
+    int autotune_grids(int nsm) {
         if (const char* e = std::getenv("LLG_B200_NO_AUTOTUNE"))
             if (e[0] == '1') return LLG_OK;
         int rc;
@@ -540,7 +574,7 @@ struct Engine final : EngineBase {
             c.erase(std::unique(c.begin(), c.end()), c.end());
             return c;
         };
-        auto tune = [&](int which, const EvalSpec& spec, int* grid, int items, int occ) -> int {
+        auto tune = [&](int which, const EvalSpec& spec, LaunchGeom& geom, int* grid, int items, int occ) -> int {
             float best = 1e30f;
             int best_g = *grid;
             for (int g : candidates(items, occ)) {
@@ -560,11 +594,15 @@ struct Engine final : EngineBase {
             *grid = best_g;
             return LLG_OK;
         };
-        const int nr = geom.n_row_items, nc = geom.n_col_items;
-        if ((rc = tune(0, stage, &geom.grid_row, nr, fb))) return rc;
-        if (any_demag && (rc = tune(1, stage, &geom.grid_col, nc, cb))) return rc;
-        if ((rc = tune(2, stage, &geom.grid_rinv, nr, ib))) return rc;
-        if ((rc = tune(2, full, &geom.grid_rfull, nr, ub))) return rc;
+        for (size_t i = 0; i < rseg.size(); ++i) {
+            LaunchGeom& sg = rseg[i];
+            const int nr = sg.n_row_items;
+            if ((rc = tune(0, stage, sg, &sg.grid_row, nr, rocc[i][0]))) return rc;
+            if ((rc = tune(2, stage, sg, &sg.grid_rinv, nr, rocc[i][1]))) return rc;
+            if ((rc = tune(2, full, sg, &sg.grid_rfull, nr, rocc[i][2]))) return rc;
+        }
+        for (size_t i = 0; i < cseg.size(); ++i)
+            if ((rc = tune(1, stage, cseg[i], &cseg[i].grid_col, cseg[i].n_col_items, cocc[i]))) return rc;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         invalidate_fsal_host();
@@ -1235,11 +1273,12 @@ struct Engine final : EngineBase {
         double acc[3] = {0, 0, 0};
         for (int r = 0; r < reps; ++r) {
             CUDA_TRY(cudaEventRecord(ev[0], stream));
-            CUDA_TRY(launch_one<R>(0, e, geom, stream));
+            for (auto& sg : rseg) CUDA_TRY(launch_one<R>(0, e, sg, stream));
             CUDA_TRY(cudaEventRecord(ev[1], stream));
-            if (e.demag && geom.any_demag) CUDA_TRY(launch_one<R>(1, e, geom, stream));
+            if (e.demag && geom.any_demag)
+                for (auto& sg : cseg) CUDA_TRY(launch_one<R>(1, e, sg, stream));
             CUDA_TRY(cudaEventRecord(ev[2], stream));
-            CUDA_TRY(launch_one<R>(2, e, geom, stream));
+            for (auto& sg : rseg) CUDA_TRY(launch_one<R>(2, e, sg, stream));
             CUDA_TRY(cudaEventRecord(ev[3], stream));
             CUDA_TRY(cudaEventSynchronize(ev[3]));
             for (int q = 0; q < 3; ++q) {
