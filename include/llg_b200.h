@@ -248,6 +248,30 @@ void llg_init_uniform_with_noise(int64_t n, const double dir[3], double noise,  
                                  uint64_t seed, double* m_aos);
 
 /* ---------------------------------------------------------------------------
+ * Demag with periodic images and the k-space kernel cache.
+ * llg_demag_op is Demag2D (demag_fft_uniform.rs:434-770) for pbc_x / pbc_y
+ * periodic images (0 = open boundary in that direction; a periodic direction is
+ * not padded: px = pbc_x ? nx : 2 nx, likewise py; px, py <= 4096), FP64.
+ * ------------------------------------------------------------------------- */
+typedef struct llg_demag_op llg_demag_op;
+/* Demag2D::new (:470-634): with a non-NULL cache_path a matching LLGDMAG v2 file is
+ * loaded (try_load_kernel_kspace, :322-429), otherwise the kernel is built
+ * (build_kernel_realspace_pbc, :941-1005, or the open builder) and written there
+ * (write_kernel_kspace, :279-319; a failed write is ignored as in the reference).
+ * *loaded (may be NULL) tells which happened. */
+int llg_demag_op_create(llg_ctx* ctx, const llg_grid* grid, int64_t pbc_x, int64_t pbc_y, const char* cache_path,
+                        int32_t* loaded, llg_demag_op** out);
+int llg_demag_op_destroy(llg_demag_op* op);
+/* compute_demag_field_pbc (demag.rs:146-156): b_aos = B_demag of Ms m (host AoS, FP64) */
+int llg_demag_op_field(llg_demag_op* op, double ms, const double* m_aos, double* b_aos);
+/* the four unscaled k-space planes (xx, xy, yy, zz): [4][py][px] complex (re, im) */
+int llg_demag_op_kspace(llg_demag_op* op, double* out);
+/* write the LLGDMAG v2 cache file (write_kernel_kspace, :279-319) */
+int llg_demag_op_save(llg_demag_op* op, const char* path);
+/* the reference's cache path for this grid (demag_cache_path, :261-277) */
+int llg_demag_cache_filename(const llg_grid* grid, int64_t pbc_x, int64_t pbc_y, char* buf, int64_t len);
+
+/* ---------------------------------------------------------------------------
  * Learned warm start.  No reference counterpart: a six-layer 3x3 convolutional
  * network (32 channels, BF16 weights and activations, FP32 accumulation on the
  * tensor cores) maps (m, inside, B_ext / 0.05 T) to a proposal m that a relax can

@@ -14,6 +14,9 @@ template <typename R>
 cudaError_t launch_fft_strided(void* data, int L, const void* tw2, long long elem_stride, int nsig_a,
                                long long stride_a, int nsig_b, long long stride_b, bool inverse, cudaStream_t s);
 
+// Unscaled FP64 k-space kernel planes [4][py][px] complex for pbc_x / pbc_y images.
+cudaError_t build_demag_kernel_pbc(int nx, int ny, double dx, double dy, double dz, int pbc_x, int pbc_y,
+                                   void* planes_out, cudaStream_t s);
 // Builds the demag kernel spectrum of an open-boundary nx x ny grid in FP64 on
 // the GPU.  khat_out: (nx+1)*(ny+1) real4 in the solver precision, scaled by
 // 1/(4 nx ny); k64_out_dev: 4*(ny+1)*(nx+1) doubles, unscaled, layout [c][ky][kx].

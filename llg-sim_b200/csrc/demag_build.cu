@@ -151,6 +151,53 @@ __global__ void k_kernel_extract(int nx, int ny, const cx<double>* __restrict__ 
     }
 }
 
+// Periodic images (build_kernel_realspace_pbc, demag_fft_uniform.rs:941-1005):
+// one warp per displacement (sx, sy) in [-sx_max, sx_max] x [-sy_max, sy_max].
+__global__ void k_kernel_displacements(int sx_max, int sy_max, double dx, double dy, double dz, double accuracy,
+                                       double* __restrict__ comp) {
+    const long long nsx = 2LL * sx_max + 1, nsy = 2LL * sy_max + 1;
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wid >= nsx * nsy) return;
+    const long long sx = wid % nsx - sx_max, sy = wid / nsx - sy_max;
+    const double rc[3] = {(double)sx * dx, (double)sy * dy, 0.0};
+    const double cell[3] = {dx, dy, dz};
+    const long long disp[3] = {sx, sy, 0};
+    double hx[3], hy[3], hz[3];
+    warp_h_from_unit_m(0, rc, cell, disp, accuracy, hx);
+    warp_h_from_unit_m(1, rc, cell, disp, accuracy, hy);
+    warp_h_from_unit_m(2, rc, cell, disp, accuracy, hz);
+    if ((threadIdx.x & 31) == 0) {
+        const double mu0 = 4.0 * kPi * 1e-7;  // params.rs:15
+        double* o = comp + wid * 4;
+        o[0] = mu0 * hx[0];
+        o[1] = mu0 * hy[0];
+        o[2] = mu0 * hy[1];
+        o[3] = mu0 * hz[2];
+    }
+}
+
+// Wrapped sums of the images into the px x py bins, per bin in the reference's
+// accumulation order (sy ascending, then sx ascending); Kxy zero on the axes.
+__global__ void k_kernel_wrap(int sx_max, int sy_max, int px, int py, const double* __restrict__ comp,
+                              cx<double>* __restrict__ planes) {
+    const long long nsx = 2LL * sx_max + 1;
+    const long long np = (long long)px * py;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < np; e += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(e % px), iy = (int)(e / px);
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        // smallest sy >= -sy_max with sy = iy (mod py)
+        long long sy0 = iy - ((iy + (long long)sy_max) / py) * py;
+        long long sx0 = ix - ((ix + (long long)sx_max) / px) * px;
+        for (long long sy = sy0; sy <= sy_max; sy += py)
+            for (long long sx = sx0; sx <= sx_max; sx += px) {
+                const double* kc = comp + ((sy + sy_max) * nsx + (sx + sx_max)) * 4;
+                for (int c = 0; c < 4; ++c) v[c] += kc[c];
+            }
+        if (ix == 0 || iy == 0) v[1] = 0.0;
+        for (int c = 0; c < 4; ++c) planes[c * np + e] = mkc(v[c], 0.0);
+    }
+}
+
 }  // namespace
 
 template <typename R>
@@ -276,6 +323,41 @@ cudaError_t build_demag_kernel(int nx, int ny, double dx, double dy, double dz, 
         err = cudaStreamSynchronize(s);
     } while (0);
     cleanup();
+    return err;
+}
+
+// Unscaled k-space kernel planes (xx, xy, yy, zz; [c][iy][ix] complex) of Demag2D::new
+// for pbc_x / pbc_y images (0 = open, padded to 2n), px = pbc_x ? nx : 2 nx.
+cudaError_t build_demag_kernel_pbc(int nx, int ny, double dx, double dy, double dz, int pbc_x, int pbc_y,
+                                   void* planes_out, cudaStream_t s) {
+    const int px = pbc_x > 0 ? nx : 2 * nx, py = pbc_y > 0 ? ny : 2 * ny;
+    const long long np = (long long)px * py;
+    const int sx_max = pbc_x == 0 ? nx - 1 : nx * pbc_x - 1;
+    const int sy_max = pbc_y == 0 ? ny - 1 : ny * pbc_y - 1;
+    const long long ndisp = (2LL * sx_max + 1) * (2LL * sy_max + 1);
+    cx<double>* planes = reinterpret_cast<cx<double>*>(planes_out);
+    double* comp = nullptr;
+    cx<double>* twx = nullptr;
+    cx<double>* twy = nullptr;
+    cudaError_t err = cudaSuccess;
+    do {
+        if ((err = cudaMalloc(&comp, sizeof(double) * 4 * (size_t)ndisp)) != cudaSuccess) break;
+        if ((err = cudaMalloc(&twx, sizeof(cx<double>) * 2 * (size_t)px)) != cudaSuccess) break;
+        if ((err = cudaMalloc(&twy, sizeof(cx<double>) * 2 * (size_t)py)) != cudaSuccess) break;
+        const long long blocks = (ndisp * 32 + 255) / 256;
+        k_kernel_displacements<<<(unsigned)blocks, 256, 0, s>>>(sx_max, sy_max, dx, dy, dz, 10.0, comp);
+        if ((err = cudaGetLastError()) != cudaSuccess) break;
+        k_kernel_wrap<<<1184, 256, 0, s>>>(sx_max, sy_max, px, py, comp, planes);
+        if ((err = cudaGetLastError()) != cudaSuccess) break;
+        if ((err = launch_twiddles(twx, 2 * px, true, s)) != cudaSuccess) break;
+        if ((err = launch_twiddles(twy, 2 * py, true, s)) != cudaSuccess) break;
+        if ((err = launch_fft_strided<double>(planes, px, twx, 1, py, px, 4, np, false, s)) != cudaSuccess) break;
+        if ((err = launch_fft_strided<double>(planes, py, twy, px, px, 1, 4, np, false, s)) != cudaSuccess) break;
+        err = cudaStreamSynchronize(s);
+    } while (0);
+    if (comp) cudaFree(comp);
+    if (twx) cudaFree(twx);
+    if (twy) cudaFree(twy);
     return err;
 }
 

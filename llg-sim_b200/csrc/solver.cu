@@ -1311,6 +1311,9 @@ struct Engine final : EngineBase {
 struct llg_ctx {
     int device;
 };
+namespace llg {
+int ctx_device(const llg_ctx* c) { return c->device; }
+}  // namespace llg
 struct llg_solver {
     std::unique_ptr<llg::EngineBase> eng;
     int device;

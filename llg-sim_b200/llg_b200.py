@@ -149,6 +149,12 @@ def lib():
             "llg_batch_relax": (C.c_int, [vp, P(_Params), i32, P(RelaxSettings), P(RelaxReport)]),
             "llg_batch_compute_energy": (C.c_int, [vp, dp, P(EnergyBreakdown)]),
             "llg_batch_launch_count": (C.c_int, [vp, P(i64)]),
+            "llg_demag_op_create": (C.c_int, [vp, P(_Grid), i64, i64, C.c_char_p, P(i32), P(vp)]),
+            "llg_demag_op_destroy": (C.c_int, [vp]),
+            "llg_demag_op_field": (C.c_int, [vp, C.c_double, dp, dp]),
+            "llg_demag_op_kspace": (C.c_int, [vp, dp]),
+            "llg_demag_op_save": (C.c_int, [vp, C.c_char_p]),
+            "llg_demag_cache_filename": (C.c_int, [P(_Grid), i64, i64, C.c_char_p, i64]),
             "llg_warmstart_param_count": (i64, []),
             "llg_warmstart_create": (C.c_int, [vp, P(C.c_float), i64, P(vp)]),
             "llg_warmstart_destroy": (C.c_int, [vp]),
@@ -480,6 +486,59 @@ def demag_field_noalloc(nx, ny, ms, m_dev_ptr, kernel_planes_dev_ptr, b_dev_ptr,
     _check(lib().llg_demag_field_noalloc(int(nx), int(ny), float(ms), C.c_void_p(m_dev_ptr),
                                          C.c_void_p(kernel_planes_dev_ptr), C.c_void_p(b_dev_ptr),
                                          C.c_void_p(stream_ptr)))
+
+
+class DemagOp:
+    """Demag2D for pbc_x / pbc_y periodic images (0 = open; demag_fft_uniform.rs:434-770),
+    FP64.  With `cache_path`, a matching LLGDMAG v2 kernel file is loaded, else the
+    kernel is built and written there; `loaded` tells which."""
+
+    def __init__(self, grid, pbc_x=0, pbc_y=0, cache_path=None, device=0):
+        self.grid, self.pbc_x, self.pbc_y = grid, int(pbc_x), int(pbc_y)
+        self.px = grid.nx if pbc_x > 0 else 2 * grid.nx
+        self.py = grid.ny if pbc_y > 0 else 2 * grid.ny
+        h = C.c_void_p()
+        ld = C.c_int32(0)
+        g = grid._c()
+        _check(lib().llg_demag_op_create(_ctx(device), C.byref(g), self.pbc_x, self.pbc_y,
+                                         None if cache_path is None else str(cache_path).encode(), C.byref(ld),
+                                         C.byref(h)))
+        self.h, self.loaded = h, bool(ld.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().llg_demag_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def field(self, ms, m):
+        """compute_demag_field_pbc (demag.rs:146-156): B_demag [n, 3] of Ms m."""
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        out = np.empty((self.grid.nx * self.grid.ny, 3))
+        _check(lib().llg_demag_op_field(self.h, float(ms), _dp(m), _dp(out)))
+        return out
+
+    def kspace(self):
+        """Unscaled kernel spectrum [4, py, px] complex (xx, xy, yy, zz)."""
+        out = np.empty(4 * self.px * self.py * 2)
+        _check(lib().llg_demag_op_kspace(self.h, _dp(out)))
+        return out.view(np.complex128).reshape(4, self.py, self.px)
+
+    def save(self, path):
+        _check(lib().llg_demag_op_save(self.h, str(path).encode()))
+
+
+def demag_cache_filename(grid, pbc_x=0, pbc_y=0):
+    """The reference's cache path for this grid (demag_cache_path, demag_fft_uniform.rs:261-277)."""
+    buf = C.create_string_buffer(512)
+    g = grid._c()
+    _check(lib().llg_demag_cache_filename(C.byref(g), int(pbc_x), int(pbc_y), buf, 512))
+    return buf.value.decode()
 
 
 class WarmStartNet:

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -300,12 +301,17 @@ void build_kernel_realspace(const orc_grid& g, int64_t px, int64_t py, int64_t p
         // build_kernel_realspace_pbc, demag_fft_uniform.rs:941-1005
         int64_t sx_max = pbc_x == 0 ? g.nx - 1 : g.nx * pbc_x - 1;
         int64_t sy_max = pbc_y == 0 ? g.ny - 1 : g.ny * pbc_y - 1;
+        const int64_t nsx = 2 * sx_max + 1, nsy = 2 * sy_max + 1;
+        std::vector<double> comp((size_t)(nsx * nsy * 4));
+        // the displacements in parallel, then the wrapped sums in the reference's order
+#pragma omp parallel for schedule(dynamic, 16) num_threads(g_threads)
+        for (int64_t q = 0; q < nsx * nsy; ++q)
+            kernel_components(g.dx, g.dy, g.dz, q % nsx - sx_max, q / nsx - sy_max, DEMAG_ACCURACY, &comp[q * 4]);
         for (int64_t sy = -sy_max; sy <= sy_max; ++sy) {
             int64_t iy = wrap_index(sy, py);
             for (int64_t sx = -sx_max; sx <= sx_max; ++sx) {
                 int64_t ix = wrap_index(sx, px);
-                double kc[4];
-                kernel_components(g.dx, g.dy, g.dz, sx, sy, DEMAG_ACCURACY, kc);
+                const double* kc = &comp[((sy + sy_max) * nsx + (sx + sx_max)) * 4];
                 for (int c = 0; c < 4; ++c) k4[c][iy * px + ix] += kc[c];
             }
         }
@@ -315,7 +321,8 @@ void build_kernel_realspace(const orc_grid& g, int64_t px, int64_t py, int64_t p
 }
 
 // ---------------------------------------------------------------------------
-// Demag operator (Demag2D, demag_fft_uniform.rs:434-770), open boundaries.
+// Demag operator (Demag2D, demag_fft_uniform.rs:434-770): open boundaries, or
+// pbc_x / pbc_y periodic images (no padding in a periodic direction).
 // ---------------------------------------------------------------------------
 struct Demag2D {
     orc_grid g;
@@ -324,13 +331,13 @@ struct Demag2D {
     std::vector<cplx> kxx, kxy, kyy, kzz;
     std::vector<cplx> mx, my, mz, bx, by, bz;
 
-    explicit Demag2D(const orc_grid& grid) : g(grid) {
-        px = 2 * g.nx;  // demag_fft_uniform.rs:477-478
-        py = 2 * g.ny;
+    explicit Demag2D(const orc_grid& grid, int64_t pbc_x = 0, int64_t pbc_y = 0) : g(grid) {
+        px = pbc_x > 0 ? g.nx : 2 * g.nx;  // demag_fft_uniform.rs:477-478
+        py = pbc_y > 0 ? g.ny : 2 * g.ny;
         fx_f = Fft1D(px, false); fx_i = Fft1D(px, true);
         fy_f = Fft1D(py, false); fy_i = Fft1D(py, true);
         std::vector<double> k4[4];
-        build_kernel_realspace(g, px, py, 0, 0, k4);
+        build_kernel_realspace(g, px, py, pbc_x, pbc_y, k4);
         std::vector<cplx>* dst[4] = {&kxx, &kxy, &kyy, &kzz};
         for (int c = 0; c < 4; ++c) {
             dst[c]->resize(px * py);
@@ -1154,6 +1161,69 @@ void orc_demag_kernel_realspace(const orc_grid* g, int64_t pbc_x, int64_t pbc_y,
     std::vector<double> k4[4];
     build_kernel_realspace(*g, px, py, pbc_x, pbc_y, k4);
     for (int c = 0; c < 4; ++c) std::memcpy(out4 + c * px * py, k4[c].data(), sizeof(double) * px * py);
+}
+
+void orc_demag_field_pbc(const orc_grid* g, double ms, int64_t pbc_x, int64_t pbc_y, const double* m,
+                         double* b_out) {
+    // compute_demag_field_pbc (demag.rs:146-156 -> demag_fft_uniform.rs:157-186)
+    Demag2D d(*g, pbc_x, pbc_y);
+    std::fill(b_out, b_out + g->nx * g->ny * 3, 0.0);
+    d.add_field(m, b_out, ms);
+}
+
+void orc_demag_kernel_kspace_pbc(const orc_grid* g, int64_t pbc_x, int64_t pbc_y, double* out) {
+    Demag2D d(*g, pbc_x, pbc_y);
+    int64_t np = d.px * d.py;
+    const std::vector<cplx>* src[4] = {&d.kxx, &d.kxy, &d.kyy, &d.kzz};
+    for (int c = 0; c < 4; ++c) std::memcpy(out + c * np * 2, src[c]->data(), sizeof(cplx) * np);
+}
+
+int orc_write_llgdmag(const orc_grid* g, int64_t pbc_x, int64_t pbc_y, const char* path) {
+    // write_kernel_kspace, demag_fft_uniform.rs:279-319: little-endian header
+    // (magic "LLGDMAG\0", version 2, nx, ny, pbc_x, pbc_y, px, py as u32; dx, dy, dz,
+    // accuracy as f64) then kxx, kxy, kyy, kzz as px*py complex (re, im) f64 each.
+    Demag2D d(*g, pbc_x, pbc_y);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return -1;
+    const char magic[8] = {'L', 'L', 'G', 'D', 'M', 'A', 'G', '\0'};
+    const uint32_t u[7] = {2u, (uint32_t)g->nx, (uint32_t)g->ny, (uint32_t)pbc_x, (uint32_t)pbc_y, (uint32_t)d.px,
+                           (uint32_t)d.py};
+    const double h[4] = {g->dx, g->dy, g->dz, DEMAG_ACCURACY};
+    std::fwrite(magic, 1, 8, f);
+    std::fwrite(u, 4, 7, f);
+    std::fwrite(h, 8, 4, f);
+    for (const std::vector<cplx>* v : {&d.kxx, &d.kxy, &d.kyy, &d.kzz})
+        std::fwrite(v->data(), sizeof(cplx), v->size(), f);
+    return std::fclose(f) == 0 ? 0 : -1;
+}
+
+void orc_demag_field_direct_pbc(const orc_grid* g, double ms, int64_t pbc_x, int64_t pbc_y, const double* m,
+                                double* b_out) {
+    // Direct circular convolution with the wrapped real-space kernel on the px x py
+    // grid (no FFT): B(i,j) = sum K((i-i') mod px, (j-j') mod py) . Ms m(i',j')
+    int64_t nx = g->nx, ny = g->ny;
+    int64_t px = pbc_x > 0 ? nx : 2 * nx, py = pbc_y > 0 ? ny : 2 * ny;
+    std::vector<double> k4[4];
+    build_kernel_realspace(*g, px, py, pbc_x, pbc_y, k4);
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+    for (int64_t j = 0; j < ny; ++j) {
+        for (int64_t i = 0; i < nx; ++i) {
+            double sx_ = 0, sy_ = 0, sz_ = 0;
+            for (int64_t jj = 0; jj < ny; ++jj) {
+                for (int64_t ii = 0; ii < nx; ++ii) {
+                    int64_t idx = wrap_index(j - jj, py) * px + wrap_index(i - ii, px);
+                    const double* mm = &m[(jj * nx + ii) * 3];
+                    double Mx = ms * mm[0], My = ms * mm[1], Mz = ms * mm[2];
+                    sx_ += k4[0][idx] * Mx + k4[1][idx] * My;
+                    sy_ += k4[1][idx] * Mx + k4[2][idx] * My;
+                    sz_ += k4[3][idx] * Mz;
+                }
+            }
+            b_out[(j * nx + i) * 3 + 0] = sx_;
+            b_out[(j * nx + i) * 3 + 1] = sy_;
+            b_out[(j * nx + i) * 3 + 2] = sz_;
+        }
+    }
 }
 
 void orc_demag_field_direct(const orc_grid* g, double ms, const double* m, double* b_out) {

@@ -115,6 +115,18 @@ void orc_demag_kernel_realspace(const orc_grid* g, int64_t pbc_x, int64_t pbc_y,
 /* direct O(N^2) real-space convolution of the same kernel (independent of any FFT) */
 void orc_demag_field_direct(const orc_grid* g, double ms, const double* m, double* b_out);
 
+/* periodic boundaries (compute_demag_field_pbc, demag.rs:146-156; kernel demag_fft_uniform.rs:941-1005):
+ * pbc_x / pbc_y image counts, 0 = open; px = pbc_x ? nx : 2 nx (likewise py) */
+void orc_demag_field_pbc(const orc_grid* g, double ms, int64_t pbc_x, int64_t pbc_y, const double* m,
+                         double* b_out);
+/* unscaled k-space kernel, 4 planes of py*px interleaved complex */
+void orc_demag_kernel_kspace_pbc(const orc_grid* g, int64_t pbc_x, int64_t pbc_y, double* out);
+/* LLGDMAG v2 k-space cache file (write_kernel_kspace, demag_fft_uniform.rs:279-319); 0 on success */
+int orc_write_llgdmag(const orc_grid* g, int64_t pbc_x, int64_t pbc_y, const char* path);
+/* direct circular convolution with the wrapped kernel (no FFT) */
+void orc_demag_field_direct_pbc(const orc_grid* g, double ms, int64_t pbc_x, int64_t pbc_y, const double* m,
+                                double* b_out);
+
 /* 1-D FFT, interleaved complex, unnormalised, forward = exp(-2 pi i k n / N) */
 void orc_fft(int64_t n, double* data, int inverse);
 

@@ -88,6 +88,11 @@ def lib():
         L.orc_demag_kernel_kspace.argtypes = [vp, dp]
         L.orc_demag_kernel_realspace.argtypes = [C.POINTER(Grid), C.c_int64, C.c_int64, dp]
         L.orc_demag_field_direct.argtypes = [C.POINTER(Grid), C.c_double, dp, dp]
+        L.orc_demag_field_pbc.argtypes = [C.POINTER(Grid), C.c_double, C.c_int64, C.c_int64, dp, dp]
+        L.orc_demag_kernel_kspace_pbc.argtypes = [C.POINTER(Grid), C.c_int64, C.c_int64, dp]
+        L.orc_write_llgdmag.argtypes = [C.POINTER(Grid), C.c_int64, C.c_int64, C.c_char_p]
+        L.orc_write_llgdmag.restype = C.c_int
+        L.orc_demag_field_direct_pbc.argtypes = [C.POINTER(Grid), C.c_double, C.c_int64, C.c_int64, dp, dp]
         L.orc_fft.argtypes = [C.c_int64, dp, C.c_int]
         L.orc_xorshift_f64.argtypes = [C.c_uint64, C.c_int64, dp]
         L.orc_init_random.argtypes = [C.c_int64, C.c_uint64, dp]
@@ -250,6 +255,39 @@ def demag_field_direct(grid, ms, m):
     m = np.ascontiguousarray(m, dtype=np.float64)
     out = np.empty((grid.nx * grid.ny, 3))
     lib().orc_demag_field_direct(C.byref(grid), float(ms), _dp(m), _dp(out))
+    return out
+
+
+def pad_sizes(grid, pbc_x, pbc_y):
+    """Padded FFT sizes of Demag2D::new (demag_fft_uniform.rs:477-478)."""
+    return (grid.nx if pbc_x > 0 else 2 * grid.nx), (grid.ny if pbc_y > 0 else 2 * grid.ny)
+
+
+def demag_field_pbc(grid, ms, pbc_x, pbc_y, m):
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    out = np.empty((grid.nx * grid.ny, 3))
+    lib().orc_demag_field_pbc(C.byref(grid), float(ms), int(pbc_x), int(pbc_y), _dp(m), _dp(out))
+    return out
+
+
+def kernel_kspace_pbc(grid, pbc_x, pbc_y):
+    """Unscaled k-space kernel planes [4, py, px] complex (xx, xy, yy, zz)."""
+    px, py = pad_sizes(grid, pbc_x, pbc_y)
+    out = np.empty(4 * px * py * 2)
+    lib().orc_demag_kernel_kspace_pbc(C.byref(grid), int(pbc_x), int(pbc_y), _dp(out))
+    return out.view(np.complex128).reshape(4, py, px)
+
+
+def write_llgdmag(grid, pbc_x, pbc_y, path):
+    rc = lib().orc_write_llgdmag(C.byref(grid), int(pbc_x), int(pbc_y), str(path).encode())
+    if rc != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def demag_field_direct_pbc(grid, ms, pbc_x, pbc_y, m):
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    out = np.empty((grid.nx * grid.ny, 3))
+    lib().orc_demag_field_direct_pbc(C.byref(grid), float(ms), int(pbc_x), int(pbc_y), _dp(m), _dp(out))
     return out
 
 

@@ -46,3 +46,12 @@ def test_warmstart_param_count_matches_reference_layout(gpu):
     import warmstart_ref
 
     assert gpu.WarmStartNet.param_count() == warmstart_ref.param_count() == 39907
+
+
+def test_demag_cache_filename_matches_reference_naming(gpu):
+    g = gpu.Grid2D(128, 32, 4e-9, 4e-9, 3e-9)
+    assert gpu.demag_cache_filename(g, 0, 0) == (
+        "out/demag_cache/demag_kernel_nx128_ny32_pbcx0_pbcy0_px256_py64_dx4.000e-9_dy4.000e-9_dz3.000e-9_acc10.00.bin")
+    g = gpu.Grid2D(2, 128, 1e-9, 1e-9, 0.5e-9)
+    assert gpu.demag_cache_filename(g, 32, 0) == (
+        "out/demag_cache/demag_kernel_nx2_ny128_pbcx32_pbcy0_px2_py256_dx1.000e-9_dy1.000e-9_dz5.000e-10_acc10.00.bin")
