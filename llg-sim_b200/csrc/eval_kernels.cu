@@ -33,6 +33,10 @@ constexpr size_t kStaticSmemCol = 64;   // mbarriers and the timeout flag of k_c
 bool lean_epilogue(const EvalSpec& e) {
     return e.err == ERR_NONE && !e.reduce && e.local && (e.rhs == RHS_LLG || e.rhs == RHS_RELAX);
 }
+// The last RK45 stage of a run (no reductions): torque plus the error norm.
+bool lean_err45_epilogue(const EvalSpec& e) {
+    return e.err == ERR_RK45 && !e.reduce && e.local && e.rhs == RHS_LLG && e.k_out != KB_NONE;
+}
 
 }  // namespace
 
@@ -95,9 +99,11 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
         if (RowCfg<R, L>::SMEM <= kSmemMax) {
             cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_row_inverse_fast<R, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_row_inverse_fast<R, L, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_row_inverse_fast<R, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_row_inverse_fast<R, L, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)RowCfg<R, L>::SMEM);
+            cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
         }
         if (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
@@ -106,8 +112,9 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
         // the whole unified L1/shared array as shared memory, so that occupancy is
         // bounded by registers and the blocks' own shared memory only
         cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(k_row_inverse_fast<R, L, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(k_row_inverse_fast<R, L, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_row_inverse_fast<R, L, 0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_row_inverse_fast<R, L, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     };
     for (int L : {16, 32, 64, 128, 256, 512, 1024, 2048}) dispatch_L<R>(L, set_all);
@@ -124,11 +131,14 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
                     if (which == 0)
                         k_row_forward_fast<R, L><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
                             g.films, g.row_items, g.n_row_items, spec);
+                    else if (lean_err45_epilogue(spec))
+                        k_row_inverse_fast<R, L, 2><<<g.grid_rinv, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                            g.films, g.row_items, g.n_row_items, spec);
                     else if (lean_epilogue(spec))
-                        k_row_inverse_fast<R, L, true><<<g.grid_rinv, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                        k_row_inverse_fast<R, L, 1><<<g.grid_rinv, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
                             g.films, g.row_items, g.n_row_items, spec);
                     else
-                        k_row_inverse_fast<R, L, false><<<g.grid_rfull, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
+                        k_row_inverse_fast<R, L, 0><<<g.grid_rfull, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
                             g.films, g.row_items, g.n_row_items, spec);
                 }
             });
@@ -173,9 +183,9 @@ void fast_occupancy(int nx, int ny, int* fwd_blocks_per_sm, int* inv_blocks_per_
             int a = 1, b = 1, c = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_row_forward_fast<R, L>, RowCfg<R, L>::THREADS,
                                                           RowCfg<R, L>::SMEM);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_row_inverse_fast<R, L, true>, RowCfg<R, L>::THREADS,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_row_inverse_fast<R, L, 1>, RowCfg<R, L>::THREADS,
                                                           RowCfg<R, L>::SMEM);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_row_inverse_fast<R, L, false>, RowCfg<R, L>::THREADS,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_row_inverse_fast<R, L, 0>, RowCfg<R, L>::THREADS,
                                                           RowCfg<R, L>::SMEM);
             *fwd_blocks_per_sm = std::max(1, a);
             *inv_blocks_per_sm = std::max(1, b);

@@ -387,8 +387,9 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
 }
 
 // ---------------------------------------------------------------------------
-template <typename R, int L, bool LEAN>
-__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((LEAN ? RowCfg<R, L>::MAXREG : RowCfg<R, L>::REGCAP)) k_row_inverse_fast(const FilmDev* __restrict__ films,
+// MODE 0: full epilogue; 1: lean stage epilogue; 2: lean + RK45 error norm.
+template <typename R, int L, int MODE>
+__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((MODE == 1 ? RowCfg<R, L>::MAXREG : RowCfg<R, L>::REGCAP)) k_row_inverse_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
                                                                             int nitems, EvalSpec spec) {
     using C = RowCfg<R, L>;
@@ -480,7 +481,8 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((LEAN ? Row
             const cx<R> z = buf[(2 * (T + r / 2)) * BUF + padi<E>(i)];
             return (r & 1) ? z.im : z.re;
         };
-        if constexpr (LEAN) row_epilogue_lean<R>(F, spec, st, w.blk, T, do_fft, dfield);
+        if constexpr (MODE == 1) row_epilogue_lean<R, false>(F, spec, st, w.blk, T, do_fft, dfield);
+        else if constexpr (MODE == 2) row_epilogue_lean<R, true>(F, spec, st, w.blk, T, do_fft, dfield);
         else row_epilogue<R>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
         __syncthreads();
     }

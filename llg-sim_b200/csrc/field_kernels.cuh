@@ -590,9 +590,11 @@ __device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& s
         }
 }
 
-// Epilogue of an intermediate RK stage: local terms + demag + torque only.
-template <typename R, typename DF>
-__device__ __forceinline__ void row_epilogue_lean(const FilmDev& F, const EvalSpec& spec, const StepState* st, int blk,
+// Epilogue of an intermediate RK stage: local terms + demag + torque only; with
+// ERR45 also the Dormand-Prince error norm of the last stage (the FP64 sums of the
+// full epilogue below, in the same order, from 16-byte vector loads of k1, k3..k6).
+template <typename R, bool ERR45 = false, typename DF>
+__device__ __forceinline__ void row_epilogue_lean(const FilmDev& F, const EvalSpec& spec, StepState* st, int blk,
                                                   int T, bool do_fft, DF dfield) {
     const int nx = F.nx, ny = F.ny, n = nx * ny;
     const int j0 = blk * T;
@@ -609,6 +611,8 @@ __device__ __forceinline__ void row_epilogue_lean(const FilmDev& F, const EvalSp
     // centre, upper and lower rows as 16-byte vectors plus the two x halos, all
     // loaded before any arithmetic
     constexpr int W = Vec16<R>::W;
+    double errmax = 0.0;
+    bool errnan = false;
     for (int e = threadIdx.x; e < T * nx / W; e += blockDim.x) {
         const int c0 = e * W, r = c0 / nx, i0 = c0 - r * nx, j = j0 + r;
         if (j >= ny) continue;
@@ -657,6 +661,45 @@ __device__ __forceinline__ void row_epilogue_lean(const FilmDev& F, const EvalSp
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) stv(kout + c * n + idx0, o3[c]);
+        if constexpr (ERR45) {
+            // eps contribution max_c |sum_q b_q k_q - sum_q bhat_q k_q| (llg.rs:948-997)
+            double th[W][3], tl[W][3];
+#pragma unroll
+            for (int l = 0; l < W; ++l)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) { th[l][c] = 0.0; tl[l][c] = 0.0; }
+#pragma unroll
+            for (int q = 1; q <= 7; ++q) {
+                const double wb = spec.wb[q], wh = spec.wh[q];
+                if (wb == 0.0 && wh == 0.0) continue;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    Vec16<R> kv = q == 7 ? o3[c] : ldv(kbuf<R>(F, q, cur) + c * n + idx0);
+#pragma unroll
+                    for (int l = 0; l < W; ++l) {
+                        th[l][c] = th[l][c] + wb * (double)kv.v[l];
+                        tl[l][c] = tl[l][c] + wh * (double)kv.v[l];
+                    }
+                }
+            }
+#pragma unroll
+            for (int l = 0; l < W; ++l) {
+                const double dm = fmax(fmax(fabs(th[l][0] - tl[l][0]), fabs(th[l][1] - tl[l][1])),
+                                       fabs(th[l][2] - tl[l][2]));
+                if (dm != dm) errnan = true;
+                else errmax = fmax(errmax, dm);
+            }
+        }
+    }
+    if constexpr (ERR45) {
+        // non-negative doubles order like their bit patterns; NaN is reported as a
+        // quiet-NaN pattern, above every finite value and +inf
+        const double v = warp_max(errmax);
+        const bool anynan = __any_sync(0xffffffffu, errnan);
+        if ((threadIdx.x & 31) == 0) {
+            unsigned long long bits = anynan ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(v);
+            atomicMax(&st->err_bits, bits);
+        }
     }
 }
 
