@@ -67,9 +67,11 @@ template <typename R>
 cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s);
 template <typename R>
 cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col);
-// Launches one pass of an evaluation: 0 = row forward, 1 = column, 2 = row inverse.
+// Launches one pass of an evaluation: 0 = row forward, 1 = column, 2 = row inverse
+// (on the register-FFT path with the streaming stage kernels around them); adds the
+// number of kernels launched to *nk when nk is not null.
 template <typename R>
-cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s);
+cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s, int* nk = nullptr);
 
 // Learned warm-start network (conv_tc.cu).
 namespace ws {

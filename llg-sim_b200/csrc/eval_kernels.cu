@@ -3,8 +3,10 @@
 // shared-memory Stockham kernels otherwise.
 #include "build_api.h"
 #include "fast_kernels.cuh"
+#include "stage_kernels.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace llg {
 
@@ -33,6 +35,10 @@ constexpr size_t kStaticSmemCol = 64;   // mbarriers and the timeout flag of k_c
 bool lean_epilogue(const EvalSpec& e) {
     return e.err == ERR_NONE && !e.reduce && e.local && (e.rhs == RHS_LLG || e.rhs == RHS_RELAX);
 }
+int stage_grid(long long work) {
+    return (int)std::max(1LL, std::min((work + 255) / 256, 148LL * 8));
+}
+
 // The last RK45 stage of a run (no reductions): torque plus the error norm.
 bool lean_err45_epilogue(const EvalSpec& e) {
     return e.err == ERR_RK45 && !e.reduce && e.local && e.rhs == RHS_LLG && e.k_out != KB_NONE;
@@ -103,8 +109,6 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
                                  (int)RowCfg<R, L>::SMEM);
             cudaFuncSetAttribute(k_row_inverse_fast<R, L, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)RowCfg<R, L>::SMEM);
         }
         if (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
             cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -114,7 +118,6 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
         cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaFuncSetAttribute(k_row_inverse_fast<R, L, 0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaFuncSetAttribute(k_row_inverse_fast<R, L, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     };
     for (int L : {16, 32, 64, 128, 256, 512, 1024, 2048}) dispatch_L<R>(L, set_all);
@@ -122,30 +125,44 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
 }
 
 template <typename R>
-cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s) {
+cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s, int* nk) {
+    int count = 0;
     if (which == 0 || which == 2) {
         if (g.fast_row) {
             dispatch_L<R>(g.fast_row, [&](auto LC) {
                 constexpr int L = decltype(LC)::value;
                 if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
-                    if (which == 0)
-                        k_row_forward_fast<R, L><<<g.grid_row, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
-                            g.films, g.row_items, g.n_row_items, spec);
-                    else if (lean_err45_epilogue(spec))
-                        k_row_inverse_fast<R, L, 2><<<g.grid_rinv, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
-                            g.films, g.row_items, g.n_row_items, spec);
-                    else if (lean_epilogue(spec))
-                        k_row_inverse_fast<R, L, 1><<<g.grid_rinv, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
-                            g.films, g.row_items, g.n_row_items, spec);
-                    else
-                        k_row_inverse_fast<R, L, 0><<<g.grid_rfull, RowCfg<R, L>::THREADS, RowCfg<R, L>::SMEM, s>>>(
-                            g.films, g.row_items, g.n_row_items, spec);
+                    using C = RowCfg<R, L>;
+                    if (which == 0) {
+                        k_row_forward_fast<R, L><<<g.grid_row, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
+                                                                                        g.n_row_items, spec);
+                        ++count;
+                    } else if (lean_epilogue(spec) || lean_err45_epilogue(spec)) {
+                        // transform only, then the torque epilogue as a streaming kernel
+                        constexpr int CPI = C::T * L;
+                        const long long cells = (long long)g.n_row_items * CPI;
+                        k_row_inverse_fast<R, L, 1><<<g.grid_rinv, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
+                                                                                            g.n_row_items, spec);
+                        if (lean_err45_epilogue(spec))
+                            k_stage_torque<R, true><<<stage_grid(cells), 256, 0, s>>>(g.films, g.row_items,
+                                                                                        g.n_row_items, CPI, spec);
+                        else
+                            k_stage_torque<R, false><<<stage_grid(cells), 256, 0, s>>>(g.films, g.row_items,
+                                                                                         g.n_row_items, CPI, spec);
+                        count += 2;
+                    } else {
+                        k_row_inverse_fast<R, L, 0><<<g.grid_rfull, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
+                                                                                             g.n_row_items, spec);
+                        ++count;
+                    }
                 }
             });
         } else if (which == 0) {
             k_row_forward<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+            ++count;
         } else {
             k_row_inverse<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+            ++count;
         }
     } else {
         if (g.fast_col) {
@@ -158,19 +175,21 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
         } else {
             k_column<R><<<g.grid_col, 256, g.smem_col, s>>>(g.films, g.col_items, g.n_col_items, spec);
         }
+        ++count;
     }
+    if (nk) *nk += count;
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s) {
-    cudaError_t e = launch_one<R>(0, spec, g, s);
+    cudaError_t e = launch_one<R>(0, spec, g, s, nullptr);
     if (e != cudaSuccess) return e;
     if (spec.demag && g.any_demag) {
-        e = launch_one<R>(1, spec, g, s);
+        e = launch_one<R>(1, spec, g, s, nullptr);
         if (e != cudaSuccess) return e;
     }
-    return launch_one<R>(2, spec, g, s);
+    return launch_one<R>(2, spec, g, s, nullptr);
 }
 
 template <typename R>
@@ -208,8 +227,8 @@ template FastCfg fast_config<float>(int, int);
 template FastCfg fast_config<double>(int, int);
 template cudaError_t build_pass_tables<float>(void*, int, void*, int, cudaStream_t);
 template cudaError_t build_pass_tables<double>(void*, int, void*, int, cudaStream_t);
-template cudaError_t launch_one<float>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t);
-template cudaError_t launch_one<double>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t);
+template cudaError_t launch_one<float>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
+template cudaError_t launch_one<double>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
 template cudaError_t prepare_eval_kernels<float>(size_t, size_t);
 template cudaError_t prepare_eval_kernels<double>(size_t, size_t);
 template cudaError_t launch_eval<float>(const EvalSpec&, const LaunchGeom&, cudaStream_t);

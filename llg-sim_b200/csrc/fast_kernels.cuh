@@ -106,33 +106,46 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((RowCfg<R, 
             cx<R>* z = c < 2 ? &buf[(2 * r) * BUF + padi<E>(i)] : &buf[(2 * (T + r / 2)) * BUF + padi<E>(i)];
             return (c == 0 || (c == 2 && (r & 1) == 0)) ? &z->re : &z->im;
         };
-#pragma unroll 1
-        for (int e = tid; e < 3 * NV; e += C::THREADS) {
-            const int c = e / NV, ev = e - c * NV;
-            const int c0 = ev * W, r = c0 / L, i0 = c0 - r * L, j = j0 + r;
-            Vec16<R> a;
+        // two vectors per thread and round: both vectors' loads are in flight before
+        // either is stored (the stores go to shared memory after the loads)
+        constexpr int U = 2;
+        for (int e0 = tid; e0 < 3 * NV; e0 += U * C::THREADS) {
+            Vec16<R> a[U];
 #pragma unroll
-            for (int l = 0; l < W; ++l) a.v[l] = (R)0;
-            if (j < ny) {
-                const int idx = c * n + j * L + i0;
-                if (spec.nterm > 0) {
-                    a = ldv(m0 + idx);
-                    Vec16<R> ka[6];
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u * C::THREADS;
+                const int c = e / NV, ev = e - c * NV;
+                const int r = (ev * W) / L, j = j0 + r;
 #pragma unroll
-                    for (int q = 0; q < 6; ++q)
-                        if (q < spec.nterm) ka[q] = ldv(kp[q] + idx);
+                for (int l = 0; l < W; ++l) a[u].v[l] = (R)0;
+                if (e < 3 * NV && j < ny) {
+                    const int idx = c * n + j * L + (ev * W - r * L);
+                    if (spec.nterm > 0) {
+                        a[u] = ldv(m0 + idx);
+                        Vec16<R> ka[6];
 #pragma unroll
-                    for (int q = 0; q < 6; ++q)
-                        if (q < spec.nterm) {
+                        for (int q = 0; q < 6; ++q)
+                            if (q < spec.nterm) ka[q] = ldv(kp[q] + idx);
 #pragma unroll
-                            for (int l = 0; l < W; ++l) a.v[l] = a.v[l] + cq[q] * ka[q].v[l];
-                        }
-                } else {
-                    a = ldv(ms + idx);
+                        for (int q = 0; q < 6; ++q)
+                            if (q < spec.nterm) {
+#pragma unroll
+                                for (int l = 0; l < W; ++l) a[u].v[l] = a[u].v[l] + cq[q] * ka[q].v[l];
+                            }
+                    } else {
+                        a[u] = ldv(ms + idx);
+                    }
                 }
             }
 #pragma unroll
-            for (int l = 0; l < W; ++l) *slot(c, r, i0 + l) = a.v[l];
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u * C::THREADS;
+                if (e >= 3 * NV) continue;
+                const int c = e / NV, ev = e - c * NV;
+                const int c0 = ev * W, r = c0 / L, i0 = c0 - r * L;
+#pragma unroll
+                for (int l = 0; l < W; ++l) *slot(c, r, i0 + l) = a[u].v[l];
+            }
         }
         __syncthreads();
         for (int e = tid; e < NV; e += C::THREADS) {
@@ -387,7 +400,8 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
 }
 
 // ---------------------------------------------------------------------------
-// MODE 0: full epilogue; 1: lean stage epilogue; 2: lean + RK45 error norm.
+// MODE 0: full epilogue; 1: no epilogue, the demag field is written to the film's
+// bdem planes for k_stage_torque.
 template <typename R, int L, int MODE>
 __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((MODE == 1 ? RowCfg<R, L>::MAXREG : RowCfg<R, L>::REGCAP)) k_row_inverse_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
@@ -481,9 +495,27 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((MODE == 1 
             const cx<R> z = buf[(2 * (T + r / 2)) * BUF + padi<E>(i)];
             return (r & 1) ? z.im : z.re;
         };
-        if constexpr (MODE == 1) row_epilogue_lean<R, false>(F, spec, st, w.blk, T, do_fft, dfield);
-        else if constexpr (MODE == 2) row_epilogue_lean<R, true>(F, spec, st, w.blk, T, do_fft, dfield);
-        else row_epilogue<R>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
+        if constexpr (MODE == 1) {
+            // demag field only, for the streaming torque kernel
+            if (do_fft) {
+                constexpr int W = Vec16<R>::W;
+                const int n = F.nx * ny;
+                R* __restrict__ bd = reinterpret_cast<R*>(F.bdem);
+                for (int e = tid; e < T * L / W; e += C::THREADS) {
+                    const int c0 = e * W, r = c0 / L, i0 = c0 - r * L, j = j0 + r;
+                    if (j >= ny) continue;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        Vec16<R> o;
+#pragma unroll
+                        for (int l = 0; l < W; ++l) o.v[l] = dfield(r, i0 + l, c);
+                        stv(bd + c * n + j * L + i0, o);
+                    }
+                }
+            }
+        } else {
+            row_epilogue<R>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
+        }
         __syncthreads();
     }
 }

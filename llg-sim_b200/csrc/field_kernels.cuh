@@ -590,116 +590,15 @@ __device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& s
         }
 }
 
-// Epilogue of an intermediate RK stage: local terms + demag + torque only; with
-// ERR45 also the Dormand-Prince error norm of the last stage (the FP64 sums of the
-// full epilogue below, in the same order, from 16-byte vector loads of k1, k3..k6).
-template <typename R, bool ERR45 = false, typename DF>
-__device__ __forceinline__ void row_epilogue_lean(const FilmDev& F, const EvalSpec& spec, StepState* st, int blk,
-                                                  int T, bool do_fft, DF dfield) {
-    const int nx = F.nx, ny = F.ny, n = nx * ny;
-    const int j0 = blk * T;
-    const int cur = st->cur;
-    const R* __restrict__ msb = mbuf<R>(F, spec.m_in, cur);
-    R* __restrict__ kout = kbuf<R>(F, spec.k_out, cur);
-    const R gam = (R)F.gamma, alp = (R)F.alpha;
-    const R denom = (R)1 + alp * alp;
-    const R pref = spec.rhs == RHS_LLG ? -gam / denom : -gam * alp / denom;
-    const R c1 = spec.rhs == RHS_LLG ? (R)1 : (R)0;
-    const R c2 = spec.rhs == RHS_LLG ? alp : (R)1;
-    const bool dmi_on = spec.dmi != 0;
-    // W consecutive cells per thread (nx is a multiple of W on this path): the
-    // centre, upper and lower rows as 16-byte vectors plus the two x halos, all
-    // loaded before any arithmetic
-    constexpr int W = Vec16<R>::W;
-    double errmax = 0.0;
-    bool errnan = false;
-    for (int e = threadIdx.x; e < T * nx / W; e += blockDim.x) {
-        const int c0 = e * W, r = c0 / nx, i0 = c0 - r * nx, j = j0 + r;
-        if (j >= ny) continue;
-        const int idx0 = j * nx + i0;
-        Vec16<R> mc3[3], up3[3], dn3[3];
-        R hl[3] = {(R)0, (R)0, (R)0}, hr[3] = {(R)0, (R)0, (R)0};
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            mc3[c] = ldv(msb + c * n + idx0);
-            up3[c] = j > 0 ? ldv(msb + c * n + idx0 - nx) : mc3[c];
-            dn3[c] = j + 1 < ny ? ldv(msb + c * n + idx0 + nx) : mc3[c];
-            if (i0 > 0) hl[c] = msb[c * n + idx0 - 1];
-            if (i0 + W < nx) hr[c] = msb[c * n + idx0 + W];
-        }
-        Vec16<R> o3[3];
-#pragma unroll
-        for (int l = 0; l < W; ++l) {
-            const int i = i0 + l;
-            R mc[3] = {mc3[0].v[l], mc3[1].v[l], mc3[2].v[l]};
-            auto nb = [&](int d, R* o) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    if (d == 0) o[c] = l > 0 ? mc3[c].v[l > 0 ? l - 1 : 0] : hl[c];
-                    else if (d == 1) o[c] = l + 1 < W ? mc3[c].v[l + 1 < W ? l + 1 : 0] : hr[c];
-                    else if (d == 2) o[c] = up3[c].v[l];
-                    else o[c] = dn3[c].v[l];
-                }
-            };
-            R b[3];
-            local_field_nb<R>(F, nb, i, j, dmi_on, mc, b);
-            if (do_fft) {
-                b[0] += dfield(r, i, 0);
-                b[1] += dfield(r, i, 1);
-                b[2] += dfield(r, i, 2);
-            }
-            // llg_rhs (llg.rs:20-32) / llg_rhs_relax (llg.rs:38-50)
-            const R t0 = mc[1] * b[2] - mc[2] * b[1];
-            const R t1 = mc[2] * b[0] - mc[0] * b[2];
-            const R t2 = mc[0] * b[1] - mc[1] * b[0];
-            const R u0 = mc[1] * t2 - mc[2] * t1;
-            const R u1 = mc[2] * t0 - mc[0] * t2;
-            const R u2 = mc[0] * t1 - mc[1] * t0;
-            o3[0].v[l] = pref * (c1 * t0 + c2 * u0);
-            o3[1].v[l] = pref * (c1 * t1 + c2 * u1);
-            o3[2].v[l] = pref * (c1 * t2 + c2 * u2);
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) stv(kout + c * n + idx0, o3[c]);
-        if constexpr (ERR45) {
-            // eps contribution max_c |sum_q b_q k_q - sum_q bhat_q k_q| (llg.rs:948-997)
-            double th[W][3], tl[W][3];
-#pragma unroll
-            for (int l = 0; l < W; ++l)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) { th[l][c] = 0.0; tl[l][c] = 0.0; }
-#pragma unroll
-            for (int q = 1; q <= 7; ++q) {
-                const double wb = spec.wb[q], wh = spec.wh[q];
-                if (wb == 0.0 && wh == 0.0) continue;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    Vec16<R> kv = q == 7 ? o3[c] : ldv(kbuf<R>(F, q, cur) + c * n + idx0);
-#pragma unroll
-                    for (int l = 0; l < W; ++l) {
-                        th[l][c] = th[l][c] + wb * (double)kv.v[l];
-                        tl[l][c] = tl[l][c] + wh * (double)kv.v[l];
-                    }
-                }
-            }
-#pragma unroll
-            for (int l = 0; l < W; ++l) {
-                const double dm = fmax(fmax(fabs(th[l][0] - tl[l][0]), fabs(th[l][1] - tl[l][1])),
-                                       fabs(th[l][2] - tl[l][2]));
-                if (dm != dm) errnan = true;
-                else errmax = fmax(errmax, dm);
-            }
-        }
-    }
-    if constexpr (ERR45) {
-        // non-negative doubles order like their bit patterns; NaN is reported as a
-        // quiet-NaN pattern, above every finite value and +inf
-        const double v = warp_max(errmax);
-        const bool anynan = __any_sync(0xffffffffu, errnan);
-        if ((threadIdx.x & 31) == 0) {
-            unsigned long long bits = anynan ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(v);
-            atomicMax(&st->err_bits, bits);
-        }
+// Warp maximum of the error norm into the film's accumulator: non-negative doubles
+// order like their bit patterns; NaN is reported as a quiet-NaN pattern, above every
+// finite value and +inf.  All lanes of the warp must call it for the same film.
+__device__ __forceinline__ void err_to_state(StepState* st, double errmax, bool errnan) {
+    const double v = warp_max(errmax);
+    const bool anynan = __any_sync(0xffffffffu, errnan);
+    if ((threadIdx.x & 31) == 0) {
+        unsigned long long bits = anynan ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(v);
+        atomicMax(&st->err_bits, bits);
     }
 }
 

@@ -320,11 +320,12 @@ struct Engine final : EngineBase {
 
     // One evaluation: row forward, column (with demag), row inverse, one launch per segment.
     int eval(const EvalSpec& e) {
-        for (auto& sg : rseg) CUDA_TRY(launch_one<R>(0, e, sg, stream));
+        int nk = 0;
+        for (auto& sg : rseg) CUDA_TRY(launch_one<R>(0, e, sg, stream, &nk));
         if (e.demag && geom.any_demag)
-            for (auto& sg : cseg) CUDA_TRY(launch_one<R>(1, e, sg, stream));
-        for (auto& sg : rseg) CUDA_TRY(launch_one<R>(2, e, sg, stream));
-        launches += 2 * (long long)rseg.size() + ((e.demag && geom.any_demag) ? (long long)cseg.size() : 0);
+            for (auto& sg : cseg) CUDA_TRY(launch_one<R>(1, e, sg, stream, &nk));
+        for (auto& sg : rseg) CUDA_TRY(launch_one<R>(2, e, sg, stream, &nk));
+        launches += nk;
         return LLG_OK;
     }
 
@@ -441,6 +442,7 @@ struct Engine final : EngineBase {
                     F.twp_col = twp_col;
                 }
                 if ((rc = dalloc(&F.X, sizeof(cx<R>) * 3 * (size_t)(nx + 1) * ny))) return rc;
+                if (frow[f] && (rc = dalloc(&F.bdem, plane))) return rc;
                 // films sharing a grid share the kernel planes (get_demag_operator, demag_fft_uniform.rs:86)
                 int same = -1;
                 for (int e = 0; e < f && same < 0; ++e)

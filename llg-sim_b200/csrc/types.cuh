@@ -84,6 +84,7 @@ struct FilmDev {
     void* ms_buf[2];              // stage-state ping-pong
     void* k[8];                   // k[1..7]; k[1]/k[7] swap with parity
     void* bout;                   // field output (RHS_FIELD)
+    void* bdem;                   // demag field planes between the split row-inverse and torque kernels
     void* X;                      // spectrum scratch
     const void* Khat;             // kernel spectrum
     const uint8_t* mask;
