@@ -100,8 +100,12 @@ __device__ __forceinline__ void cp3(const R* a, R* o) {
 // (exchange.rs:45-222), anisotropy (anisotropy.rs:10-26), DMI (dmi.rs:67-209),
 // accumulated in that order.  With a geometry mask this is the _geom variant
 // (mod.rs:78-101).
-// Neighbour values come from `nb(dir, out)`, dir 0..3 = (i-1, i+1, j-1, j+1);
-// it is called only for neighbours inside the film.
+// Neighbour values come from `nb(dir, out)`, dir 0..3 = (i-1, i+1, j-1, j+1); it
+// is called only for neighbours inside the film, once each: exchange and DMI share
+// the loaded values and differ only in their boundary rules (an edge or vacuum
+// neighbour is a chiral ghost for exchange when D != 0, else a copy of the centre;
+// for DMI an edge neighbour is a ghost and a vacuum neighbour a copy).  Divisions
+// by dx^2 and 2 dx are products with reciprocals formed in FP64 on the host.
 template <typename R, typename NB>
 __device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i, int j, bool dmi_on, const R* mc,
                                                R* b) {
@@ -110,37 +114,44 @@ __device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i,
     b[1] = (R)0 + (R)F.bext[1];
     b[2] = (R)0 + (R)F.bext[2];
     const bool in_c = cell_inside(F, idx);
-    const R dx = (R)F.dx, dy = (R)F.dy;
-    if (F.exch != 0.0 && in_c) {
+    const bool want_ex = F.exch != 0.0 && in_c, want_dmi = dmi_on && F.dmi_avail && in_c;
+    R rim[3], rip[3], rjm[3], rjp[3];
+    bool vim = false, vip = false, vjm = false, vjp = false;
+    if (want_ex || want_dmi) {
+        vim = nx > 1 && i > 0 && cell_inside(F, idx - 1);
+        vip = nx > 1 && i < nx - 1 && cell_inside(F, idx + 1);
+        vjm = ny > 1 && j > 0 && cell_inside(F, idx - nx);
+        vjp = ny > 1 && j < ny - 1 && cell_inside(F, idx + nx);
+        if (vim) nb(0, rim);
+        if (vip) nb(1, rip);
+        if (vjm) nb(2, rjm);
+        if (vjp) nb(3, rjp);
+    }
+    const R dx = (R)F.dx, dy = (R)F.dy, eta = (R)F.eta;
+    if (want_ex) {
+        // exchange.rs:45-222 with the ghosts of :8-36
         const bool he = F.has_eta != 0;
-        const R eta = (R)F.eta;
         R mim[3], mip[3], mjm[3], mjp[3];
-        if (nx == 1) cp3(mc, mim);
-        else if (i == 0) { if (he) ghost_x(mc, (R)-1, eta, dx, mim); else cp3(mc, mim); }
-        else if (!cell_inside(F, idx - 1)) { if (he) ghost_x(mc, (R)-1, eta, dx, mim); else cp3(mc, mim); }
-        else nb(0, mim);
-        if (nx == 1) cp3(mc, mip);
-        else if (i == nx - 1) { if (he) ghost_x(mc, (R)1, eta, dx, mip); else cp3(mc, mip); }
-        else if (!cell_inside(F, idx + 1)) { if (he) ghost_x(mc, (R)1, eta, dx, mip); else cp3(mc, mip); }
-        else nb(1, mip);
-        if (ny == 1) cp3(mc, mjm);
-        else if (j == 0) { if (he) ghost_y(mc, (R)-1, eta, dy, mjm); else cp3(mc, mjm); }
-        else if (!cell_inside(F, idx - nx)) { if (he) ghost_y(mc, (R)-1, eta, dy, mjm); else cp3(mc, mjm); }
-        else nb(2, mjm);
-        if (ny == 1) cp3(mc, mjp);
-        else if (j == ny - 1) { if (he) ghost_y(mc, (R)1, eta, dy, mjp); else cp3(mc, mjp); }
-        else if (!cell_inside(F, idx + nx)) { if (he) ghost_y(mc, (R)1, eta, dy, mjp); else cp3(mc, mjp); }
-        else nb(3, mjp);
-        const R coeff = (R)F.exch;
-        const R dx2 = dx * dx, dy2 = dy * dy;
+        if (nx == 1) { cp3(mc, mim); cp3(mc, mip); }
+        else {
+            if (vim) cp3(rim, mim); else if (he) ghost_x(mc, (R)-1, eta, dx, mim); else cp3(mc, mim);
+            if (vip) cp3(rip, mip); else if (he) ghost_x(mc, (R)1, eta, dx, mip); else cp3(mc, mip);
+        }
+        if (ny == 1) { cp3(mc, mjm); cp3(mc, mjp); }
+        else {
+            if (vjm) cp3(rjm, mjm); else if (he) ghost_y(mc, (R)-1, eta, dy, mjm); else cp3(mc, mjm);
+            if (vjp) cp3(rjp, mjp); else if (he) ghost_y(mc, (R)1, eta, dy, mjp); else cp3(mc, mjp);
+        }
+        const R coeff = (R)F.exch, ix2 = (R)F.inv_dx2, iy2 = (R)F.inv_dy2;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            R d2x = nx > 1 ? (mip[c] - (R)2 * mc[c] + mim[c]) / dx2 : (R)0;
-            R d2y = ny > 1 ? (mjp[c] - (R)2 * mc[c] + mjm[c]) / dy2 : (R)0;
+            R d2x = nx > 1 ? (mip[c] - (R)2 * mc[c] + mim[c]) * ix2 : (R)0;
+            R d2y = ny > 1 ? (mjp[c] - (R)2 * mc[c] + mjm[c]) * iy2 : (R)0;
             b[c] += coeff * (d2x + d2y);
         }
     }
     if (F.anis != 0.0) {
+        // anisotropy.rs:10-26
         const R coeff = (R)F.anis;
         const R u0 = (R)F.u[0], u1 = (R)F.u[1], u2 = (R)F.u[2];
         R mdotu = mc[0] * u0 + mc[1] * u1 + mc[2] * u2;
@@ -148,32 +159,24 @@ __device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i,
         b[1] += coeff * mdotu * u1;
         b[2] += coeff * mdotu * u2;
     }
-    if (dmi_on && F.dmi_avail && in_c) {
-        const R eta = (R)F.eta;
+    if (want_dmi) {
+        // dmi.rs:67-209 with the ghosts of :19-52
         R mim[3], mip[3], mjm[3], mjp[3];
         if (nx == 1) { cp3(mc, mim); cp3(mc, mip); }
         else {
-            if (i == 0) ghost_x(mc, (R)-1, eta, dx, mim);
-            else if (cell_inside(F, idx - 1)) nb(0, mim);
-            else cp3(mc, mim);
-            if (i == nx - 1) ghost_x(mc, (R)1, eta, dx, mip);
-            else if (cell_inside(F, idx + 1)) nb(1, mip);
-            else cp3(mc, mip);
+            if (i == 0) ghost_x(mc, (R)-1, eta, dx, mim); else if (vim) cp3(rim, mim); else cp3(mc, mim);
+            if (i == nx - 1) ghost_x(mc, (R)1, eta, dx, mip); else if (vip) cp3(rip, mip); else cp3(mc, mip);
         }
         if (ny == 1) { cp3(mc, mjm); cp3(mc, mjp); }
         else {
-            if (j == 0) ghost_y(mc, (R)-1, eta, dy, mjm);
-            else if (cell_inside(F, idx - nx)) nb(2, mjm);
-            else cp3(mc, mjm);
-            if (j == ny - 1) ghost_y(mc, (R)1, eta, dy, mjp);
-            else if (cell_inside(F, idx + nx)) nb(3, mjp);
-            else cp3(mc, mjp);
+            if (j == 0) ghost_y(mc, (R)-1, eta, dy, mjm); else if (vjm) cp3(rjm, mjm); else cp3(mc, mjm);
+            if (j == ny - 1) ghost_y(mc, (R)1, eta, dy, mjp); else if (vjp) cp3(rjp, mjp); else cp3(mc, mjp);
         }
-        const R pref = (R)F.dmi_pref;
-        R dmz_dx = nx > 1 ? (mip[2] - mim[2]) / ((R)2 * dx) : (R)0;
-        R dmz_dy = ny > 1 ? (mjp[2] - mjm[2]) / ((R)2 * dy) : (R)0;
-        R dmx_dx = nx > 1 ? (mip[0] - mim[0]) / ((R)2 * dx) : (R)0;
-        R dmy_dy = ny > 1 ? (mjp[1] - mjm[1]) / ((R)2 * dy) : (R)0;
+        const R pref = (R)F.dmi_pref, hx = (R)F.half_inv_dx, hy = (R)F.half_inv_dy;
+        R dmz_dx = nx > 1 ? (mip[2] - mim[2]) * hx : (R)0;
+        R dmz_dy = ny > 1 ? (mjp[2] - mjm[2]) * hy : (R)0;
+        R dmx_dx = nx > 1 ? (mip[0] - mim[0]) * hx : (R)0;
+        R dmy_dy = ny > 1 ? (mjp[1] - mjm[1]) * hy : (R)0;
         b[0] += pref * dmz_dx;
         b[1] += pref * dmz_dy;
         b[2] += -pref * (dmx_dx + dmy_dy);

@@ -396,6 +396,10 @@ struct Engine final : EngineBase {
             F.dmi_avail = (m[f].has_dmi && m[f].dmi != 0.0 && m[f].ms != 0.0 && m[f].a_ex != 0.0) ? 1 : 0;
             F.dmi_pref = F.dmi_avail ? 2.0 * m[f].dmi / m[f].ms : 0.0;
             F.anis = (m[f].k_u != 0.0 && m[f].ms != 0.0) ? 2.0 * m[f].k_u / m[f].ms : 0.0;
+            F.inv_dx2 = 1.0 / (g[f].dx * g[f].dx);
+            F.inv_dy2 = 1.0 / (g[f].dy * g[f].dy);
+            F.half_inv_dx = 0.5 / g[f].dx;
+            F.half_inv_dy = 0.5 / g[f].dy;
             for (int c = 0; c < 3; ++c) F.u[c] = m[f].easy_axis[c];
             F.demag_mat = m[f].demag ? 1 : 0;
             F.plan_row = make_plan(nx);

@@ -73,6 +73,8 @@ struct FilmDev {
     int dmi_avail;                // Material::dmi is Some and DMI field term can run
     double dmi_pref;              // 2D/Ms
     double anis;                  // 2Ku/Ms  (0 = anisotropy off)
+    double inv_dx2, inv_dy2;      // 1/dx^2, 1/dy^2 (exchange Laplacian)
+    double half_inv_dx, half_inv_dy;   // 1/(2dx), 1/(2dy) (DMI central differences)
     double u[3];
     double bext[3];
     double gamma, alpha;
