@@ -158,3 +158,27 @@ def holey_film_batch(n, size=128, seed=5):
                           b_ext=(b * math.cos(ang), b * math.sin(ang), 0.0), alpha=0.5))
     relax = dict(dt0=1e-13, torque_threshold=1e-6, max_err=1e-5, headroom=0.8, dt_min=1e-18, dt_max=1e-11)
     return films, relax
+
+
+# ---------------------------------------------------------------------------------------------
+
+def film_cost(f):
+    """Work estimate of one film per step: cells plus its padded transforms,
+    2nx x 2ny x log2(2nx x 2ny) (the demag FFTs dominate)."""
+    px, py = 2 * f.nx, 2 * f.ny
+    return float(f.n) + float(px * py) * math.log2(max(px * py, 2))
+
+
+def partition_films(films, world, rank):
+    """Indices of the films rank `rank` of `world` advances: greedy longest-first
+    assignment to the least-loaded rank (ties to the lower rank), so every film is
+    taken by exactly one rank and loads are balanced by film_cost."""
+    order = sorted(range(len(films)), key=lambda i: (-film_cost(films[i]), i))
+    load = [0.0] * world
+    owner = [0] * len(films)
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += film_cost(films[i])
+    return [i for i in range(len(films)) if owner[i] == rank]
+
