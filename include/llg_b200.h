@@ -101,6 +101,31 @@ typedef struct llg_relax_report {
     double final_torque, final_torque_max, final_max_err, final_dt;
 } llg_relax_report;
 
+/* MinimizeSettings (minimize.rs:20-63); the Option<f64> fields dm_stop,
+ * dm_torque_gate and dm_torque_gate_max as has_* flags.  `parallel` and
+ * `print_every` (minimize.rs:57-62) change neither the result nor the report
+ * and are not carried; `reserved` must be 0. */
+typedef struct llg_minimize_settings {
+    double torque_threshold;
+    int64_t max_iters;
+    double lambda0, lambda_min, lambda_max, grow, shrink;
+    int64_t stall_iters;
+    double stall_rel;
+    int64_t min_iters_before_stall;
+    int32_t has_dm_stop, has_dm_torque_gate, has_dm_torque_gate_max, reserved;
+    double dm_stop;
+    int64_t dm_samples;
+    double dm_torque_gate, dm_torque_gate_max;
+    int64_t dm_min_iters;
+} llg_minimize_settings;
+
+/* MinimizeReport, minimize.rs:94-104 */
+typedef struct llg_minimize_report {
+    int64_t iters;
+    int32_t converged, stalled, dm_converged, reserved;
+    double final_torque, final_max_dm, final_tmean, final_lambda;
+} llg_minimize_report;
+
 /* EnergyBreakdown, energy.rs:22-28 (Joule) */
 typedef struct llg_energy_breakdown {
     double exchange, anisotropy, zeeman, dmi, demag;
@@ -169,6 +194,15 @@ int llg_relax(llg_solver* s, llg_params* params, int32_t field_mask, llg_relax_s
               llg_relax_report* report);
 void llg_default_relax_settings(llg_relax_settings* st); /* impl Default, relax.rs:107-141 */
 
+/* minimize_damping_only (minimize.rs:107-369): damping-only descent
+ * m <- normalize(m + lambda (m x B) x m), one effective-field build per
+ * iteration, with the reference's lambda controller, torque threshold, dM stop
+ * and stall test, run as a device-resident loop.  params->dt is not used or
+ * changed; the resident state is updated in place. */
+int llg_minimize(llg_solver* s, const llg_params* params, int32_t field_mask, const llg_minimize_settings* settings,
+                 llg_minimize_report* report);
+void llg_default_minimize_settings(llg_minimize_settings* st); /* impl Default, minimize.rs:65-92 */
+
 /* compute_energy / compute_energy_geom (energy.rs:66-285) at the resident state. */
 int llg_compute_energy(llg_solver* s, const double b_ext[3], llg_energy_breakdown* out);
 /* torque_metric_rebuild (relax.rs:192-203): field rebuild + metric, FP64 reduction. */
@@ -208,6 +242,9 @@ int llg_batch_run_rk45(llg_batch* b, llg_params* params, int32_t field_mask, dou
 /* relax_with_report (relax.rs:334-768) for every film, driven by a device-side controller */
 int llg_batch_relax(llg_batch* b, llg_params* params, int32_t field_mask, const llg_relax_settings* settings,
                     llg_relax_report* reports);
+/* minimize_damping_only (minimize.rs:107-369) for every film, one report per film */
+int llg_batch_minimize(llg_batch* b, const llg_params* params, int32_t field_mask,
+                       const llg_minimize_settings* settings, llg_minimize_report* reports);
 int llg_batch_compute_energy(llg_batch* b, const double* b_ext /* 3*nfilms */, llg_energy_breakdown* out);
 int llg_batch_launch_count(llg_batch* b, int64_t* out);
 

@@ -95,7 +95,9 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
     cudaError_t e;
     e = cudaFuncSetAttribute(k_row_forward<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_row_inverse<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row);
+    e = cudaFuncSetAttribute(k_row_inverse<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_row_inverse<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_col);
     if (e != cudaSuccess) return e;
@@ -109,6 +111,8 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
                                  (int)RowCfg<R, L>::SMEM);
             cudaFuncSetAttribute(k_row_inverse_fast<R, L, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
+            cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)RowCfg<R, L>::SMEM);
         }
         if (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
             cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -118,6 +122,7 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
         cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaFuncSetAttribute(k_row_inverse_fast<R, L, 0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaFuncSetAttribute(k_row_inverse_fast<R, L, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     };
     for (int L : {16, 32, 64, 128, 256, 512, 1024, 2048}) dispatch_L<R>(L, set_all);
@@ -150,6 +155,10 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
                             k_stage_torque<R, false><<<stage_grid(cells), 256, 0, s>>>(g.films, g.row_items,
                                                                                          g.n_row_items, CPI, spec);
                         count += 2;
+                    } else if (spec.rhs == RHS_MINIMIZE) {
+                        k_row_inverse_fast<R, L, 2><<<g.grid_rfull, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
+                                                                                             g.n_row_items, spec);
+                        ++count;
                     } else {
                         k_row_inverse_fast<R, L, 0><<<g.grid_rfull, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
                                                                                              g.n_row_items, spec);
@@ -161,7 +170,12 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
             k_row_forward<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
             ++count;
         } else {
-            k_row_inverse<R><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items, spec);
+            if (spec.rhs == RHS_MINIMIZE)
+                k_row_inverse<R, true><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items,
+                                                                           spec);
+            else
+                k_row_inverse<R, false><<<g.grid_row, 256, g.smem_row, s>>>(g.films, g.row_items, g.n_row_items,
+                                                                            spec);
             ++count;
         }
     } else {

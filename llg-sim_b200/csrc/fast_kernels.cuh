@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
 
 // ---------------------------------------------------------------------------
 // MODE 0: full epilogue; 1: no epilogue, the demag field is written to the film's
-// bdem planes for k_stage_torque.
+// bdem planes for k_stage_torque; 2: the minimiser epilogue (RHS_MINIMIZE).
 template <typename R, int L, int MODE>
 __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((MODE == 1 ? RowCfg<R, L>::MAXREG : RowCfg<R, L>::REGCAP)) k_row_inverse_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((MODE == 1 
                 }
             }
         } else {
-            row_epilogue<R>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
+            row_epilogue<R, MODE == 2>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
         }
         __syncthreads();
     }

@@ -434,8 +434,10 @@ __global__ void __launch_bounds__(256) k_column(const FilmDev* __restrict__ film
 
 // Per-cell epilogue of the row-inverse pass (shared by the generic and the
 // register-FFT kernels): local terms, demag from dfield(r, i, c), torque,
-// stage torque store, RK error norm and FP64 block reductions.
-template <typename R, typename DF>
+// stage torque store, RK error norm and FP64 block reductions.  MIN selects the
+// minimiser update (RHS_MINIMIZE) instead; it is a separate instantiation so
+// that the integrator kernels keep their register budget.
+template <typename R, bool MIN, typename DF>
 __device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& spec, StepState* st, int blk, int T,
                                              bool do_fft, DF dfield, double* sm_red) {
     const int nx = F.nx, ny = F.ny, n = nx * ny;
@@ -444,6 +446,7 @@ __device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& s
         const R* __restrict__ msb = mbuf<R>(F, spec.m_in, cur);
         R* __restrict__ kout = spec.k_out != KB_NONE ? kbuf<R>(F, spec.k_out, cur) : nullptr;
         R* __restrict__ bout = reinterpret_cast<R*>(F.bout);
+        R* __restrict__ mout = MIN ? mbuf<R>(F, MB_M7, cur) : nullptr;
         const R gam = (R)F.gamma, alp = (R)F.alpha;
         const double dt = st->dt;
         double red[RED_NSLOT];
@@ -518,6 +521,29 @@ __device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& s
                 red[RED_MY] += (double)mc[1];
                 red[RED_MZ] += (double)mc[2];
             }
+            if constexpr (MIN) {
+                // damping-only descent update in FP64 (minimize.rs:221-254):
+                // d = (m x B) x m, m' = normalize(m + lambda d), dM = |m' - m| of the stored values
+                const double m0 = (double)mc[0], m1 = (double)mc[1], m2 = (double)mc[2];
+                const double b0 = (double)b[0], b1 = (double)b[1], b2 = (double)b[2];
+                const double q0 = m1 * b2 - m2 * b1, q1 = m2 * b0 - m0 * b2, q2 = m0 * b1 - m1 * b0;
+                const double lam = st->lam;
+                double x = m0 + lam * (q1 * m2 - q2 * m1);
+                double y = m1 + lam * (q2 * m0 - q0 * m2);
+                double z = m2 + lam * (q0 * m1 - q1 * m0);
+                const double n2 = x * x + y * y + z * z;
+                if (n2 > 0.0) {
+                    const double inv = 1.0 / sqrt(n2);
+                    x *= inv;
+                    y *= inv;
+                    z *= inv;
+                }
+                const R xs = (R)x, ys = (R)y, zs = (R)z;
+                mout[idx] = xs; mout[n + idx] = ys; mout[2 * n + idx] = zs;
+                const double ex = (double)xs - m0, ey = (double)ys - m1, ez = (double)zs - m2;
+                // max dM through the error-norm accumulator (an order-independent max)
+                errmax = fmax(errmax, sqrt(ex * ex + ey * ey + ez * ez));
+            }
             if (spec.err == ERR_RK45) {
                 // eps contribution: max_c |sum b_q k_q - sum bhat_q k_q| (llg.rs:948-997), FP64
                 double th[3] = {0.0, 0.0, 0.0}, tl[3] = {0.0, 0.0, 0.0};
@@ -574,7 +600,7 @@ __device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& s
                 }
             }
         }
-        if (spec.err != ERR_NONE) {
+        if (MIN || spec.err != ERR_NONE) {
             // non-negative doubles order like their bit patterns; NaN is reported
             // as a quiet-NaN pattern, above every finite value and +inf
             const double v = warp_max(errmax);
@@ -608,7 +634,7 @@ __device__ __forceinline__ void err_to_state(StepState* st, double errmax, bool 
 // ---------------------------------------------------------------------------
 // Pass 3: C2R along x + local terms + torque + error norm + reductions.
 // ---------------------------------------------------------------------------
-template <typename R>
+template <typename R, bool MIN>
 __global__ void __launch_bounds__(256) k_row_inverse(const FilmDev* __restrict__ films,
                                                      const WorkItem* __restrict__ items, int nitems, EvalSpec spec) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -668,7 +694,7 @@ __global__ void __launch_bounds__(256) k_row_inverse(const FilmDev* __restrict__
             __syncthreads();
         }
         auto dfield = [&](int r, int i, int c) -> R { return D[(r * 3 + c) * L + i]; };
-        row_epilogue<R>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
+        row_epilogue<R, MIN>(F, spec, st, w.blk, T, do_fft, dfield, sm_red);
         __syncthreads();
     }
 }

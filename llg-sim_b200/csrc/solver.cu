@@ -24,6 +24,7 @@
 #include "build_api.h"
 #include "field_kernels.cuh"
 #include "relax_dev.cuh"
+#include "minimize_dev.cuh"
 
 namespace llg {
 
@@ -66,7 +67,7 @@ constexpr double B1 = 2.0 / 9.0, B2 = 1.0 / 3.0, B3 = 4.0 / 9.0;
 constexpr double BH1 = 7.0 / 24.0, BH2 = 1.0 / 4.0, BH3 = 1.0 / 3.0, BH4 = 1.0 / 8.0;
 }  // namespace bs3
 
-enum { KIND_RK45 = 1, KIND_RK23 = 2, KIND_RELAX = 3 };
+enum { KIND_RK45 = 1, KIND_RK23 = 2, KIND_RELAX = 3, KIND_MINIMIZE = 4 };
 
 // Shared controller settings; per-film dt and FSAL invalidation come as FilmCtl.
 struct Control {
@@ -238,6 +239,8 @@ struct EngineBase {
                     int64_t n_acc, double t_end, int64_t max_attempts, int64_t* acc_out, int64_t* rej_out,
                     double* t_adv) = 0;
     virtual int relax(llg_params* p, int fmask, const llg_relax_settings* st, llg_relax_report* rep) = 0;
+    virtual int minimize(const llg_params* p, int fmask, const llg_minimize_settings* st,
+                         llg_minimize_report* rep) = 0;
     virtual int energy(const double* bext3n, llg_energy_breakdown* out) = 0;
     virtual int torque_metric(const llg_params* p, int fmask, int metric, double* out) = 0;
     virtual int kernel_kspace(int f, double* out) = 0;
@@ -267,6 +270,8 @@ struct Engine final : EngineBase {
     StepState* h_states = nullptr;     // pinned
     RelaxStateDev* d_relax = nullptr;
     RelaxStateDev* h_relax = nullptr;  // pinned
+    MinimizeStateDev* d_min = nullptr;
+    MinimizeStateDev* h_min = nullptr; // pinned
     FilmCtl* d_ctl = nullptr;
     FilmCtl* h_ctl = nullptr;          // pinned
     WorkItem* d_row_items = nullptr;
@@ -288,6 +293,7 @@ struct Engine final : EngineBase {
     bool l2_window = false;
     cudaStreamAttrValue l2_attr{};
     RelaxSettingsDev relax_graph_settings{};
+    MinimizeSettingsDev minimize_graph_settings{};
     // launch segments: films grouped by the row (rseg) / column (cseg) kernel they use,
     // with the resident blocks per SM of each segment's kernels
     std::vector<LaunchGeom> rseg, cseg;
@@ -304,6 +310,7 @@ struct Engine final : EngineBase {
         for (void* p : allocs) cudaFree(p);
         if (h_states) cudaFreeHost(h_states);
         if (h_relax) cudaFreeHost(h_relax);
+        if (h_min) cudaFreeHost(h_min);
         if (h_ctl) cudaFreeHost(h_ctl);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
@@ -342,6 +349,7 @@ struct Engine final : EngineBase {
         stream = own_stream;
         CUDA_TRY(cudaMallocHost(&h_states, sizeof(StepState) * nf));
         CUDA_TRY(cudaMallocHost(&h_relax, sizeof(RelaxStateDev) * nf));
+        CUDA_TRY(cudaMallocHost(&h_min, sizeof(MinimizeStateDev) * nf));
         CUDA_TRY(cudaMallocHost(&h_ctl, sizeof(FilmCtl) * nf));
         // kernel choice per film and pass: register-FFT row kernels where nx has one,
         // register-FFT column kernel where ny has one; the generic kernels otherwise.
@@ -369,6 +377,7 @@ struct Engine final : EngineBase {
         if ((rc = dalloc(&d_states, sizeof(StepState) * nf))) return rc;
         CUDA_TRY(cudaMemsetAsync(d_states, 0, sizeof(StepState) * nf, stream));
         if ((rc = dalloc(&d_relax, sizeof(RelaxStateDev) * nf))) return rc;
+        if ((rc = dalloc(&d_min, sizeof(MinimizeStateDev) * nf))) return rc;
         if ((rc = dalloc(&d_ctl, sizeof(FilmCtl) * nf))) return rc;
         std::map<int, std::vector<WorkItem>> rows_by, cols_by;   // segment key: L of the fast kernel, 0 generic
         for (int f = 0; f < nf; ++f) {
@@ -888,6 +897,21 @@ struct Engine final : EngineBase {
         return LLG_OK;
     }
 
+    // One minimiser iteration: the RHS_MINIMIZE evaluation, the reductions, the controller.
+    int launch_minimize_iteration(int fmask, const MinimizeSettingsDev& S) {
+        int rc;
+        EvalSpec e = base_spec(fmask);
+        e.req = REQ_MINIMIZE;
+        e.rhs = RHS_MINIMIZE;
+        e.reduce = 1;
+        if ((rc = eval(e))) return rc;
+        if ((rc = finalize(REQ_MINIMIZE))) return rc;
+        k_minimize_control<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, d_min, nf, S);
+        CUDA_TRY(cudaGetLastError());
+        launches += 1;
+        return LLG_OK;
+    }
+
     int graph_launch(long long key, cudaGraphExec_t ge) {
         CUDA_TRY(cudaGraphLaunch(ge, stream));
         launches += graph_kernels[key];
@@ -1156,6 +1180,87 @@ struct Engine final : EngineBase {
             p[f].dt = s.dt;
         }
         note_fsal(KIND_RK23, fmask, p);
+        return LLG_OK;
+    }
+
+    // minimize_damping_only (minimize.rs:107-369) for every film, device resident:
+    // graphs of minimiser iterations replayed until every film has finished.
+    int minimize(const llg_params* p, int fmask, const llg_minimize_settings* st, llg_minimize_report* rep) override {
+        if (fmask < 0 || fmask > 2) return set_error(LLG_ERR_INVALID, "bad field mask %d", fmask);
+        int rc;
+        if ((rc = apply_params(p))) return rc;
+        MinimizeSettingsDev S{};
+        S.thr = st->torque_threshold;
+        S.lambda0 = st->lambda0;
+        S.lambda_min = st->lambda_min;
+        S.lambda_max = st->lambda_max;
+        S.grow = st->grow;
+        S.shrink = st->shrink;
+        S.stall_rel = st->stall_rel;
+        S.dm_stop = st->dm_stop;
+        S.gate = st->dm_torque_gate;
+        S.gate_max = st->dm_torque_gate_max;
+        S.max_iters = st->max_iters;
+        S.stall_iters = st->stall_iters;
+        S.min_iters_before_stall = st->min_iters_before_stall;
+        S.dm_samples = st->dm_samples;
+        S.dm_min_iters = st->dm_min_iters;
+        S.has_dm_stop = st->has_dm_stop;
+        S.has_gate = st->has_dm_torque_gate;
+        S.has_gate_max = st->has_dm_torque_gate_max;
+        for (int f = 0; f < nf; ++f) minimize_state_init(h_min[f], S, (double)cells(f));
+        CUDA_TRY(cudaMemcpyAsync(d_min, h_min, sizeof(MinimizeStateDev) * nf, cudaMemcpyHostToDevice, stream));
+        // the state changes: every FSAL torque and cached field goes stale
+        std::unique_ptr<bool[]> inv(new bool[nf]);
+        for (int f = 0; f < nf; ++f) inv[f] = true;
+        invalidate_fsal_host();
+        if ((rc = set_control(idle_control(), nullptr, inv.get(), true))) return rc;
+        k_minimize_begin<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, d_min, nf);
+        CUDA_TRY(cudaGetLastError());
+        launches += 1;
+        const int reps = 8;
+        const long long key = graph_key(KIND_MINIMIZE, fmask, reps);
+        // the graph bakes the settings into the controller launches: rebuild when they differ
+        if (graphs.count(key) && std::memcmp(&minimize_graph_settings, &S, sizeof(S)) != 0) {
+            cudaGraphExecDestroy(graphs[key]);
+            cudaGraphDestroy(graph_defs[key]);
+            graphs.erase(key);
+            graph_defs.erase(key);
+        }
+        minimize_graph_settings = S;
+        cudaGraphExec_t ge = nullptr;
+        if ((rc = get_graph(key, reps, [&]() { return launch_minimize_iteration(fmask, S); }, &ge))) return rc;
+        // every film finishes within max_iters iterations; the bound is a safety net
+        const long long bound = std::max<long long>(st->max_iters, 0) + 4 * reps;
+        long long iters = 0;
+        int per_poll = 1;
+        bool all = true;
+        for (int f = 0; f < nf; ++f) all &= h_min[f].done != 0;
+        while (!all) {
+            for (int q = 0; q < per_poll; ++q)
+                if ((rc = graph_launch(key, ge))) return rc;
+            iters += (long long)per_poll * reps;
+            per_poll = std::min(per_poll * 2, 8);
+            CUDA_TRY(cudaMemcpyAsync(h_min, d_min, sizeof(MinimizeStateDev) * nf, cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+            all = true;
+            for (int f = 0; f < nf; ++f) all &= h_min[f].done != 0;
+            if (!all && iters > bound)
+                return set_error(LLG_ERR_TIMEOUT, "minimize did not finish within %lld iterations", bound);
+        }
+        for (int f = 0; f < nf; ++f) {
+            const MinimizeStateDev& M = h_min[f];
+            rep[f].iters = M.iters;
+            rep[f].converged = M.converged;
+            rep[f].stalled = M.stalled;
+            rep[f].dm_converged = M.dm_converged;
+            rep[f].reserved = 0;
+            rep[f].final_torque = M.final_torque;
+            rep[f].final_max_dm = M.final_max_dm;
+            rep[f].final_tmean = M.final_tmean;
+            rep[f].final_lambda = M.final_lambda;
+        }
+        invalidate_fsal_host();
         return LLG_OK;
     }
 
@@ -1485,6 +1590,33 @@ int llg_relax(llg_solver* s, llg_params* p, int32_t fmask, llg_relax_settings* s
     if (!rc) st->max_err = rep->final_max_err;  // written back as relax_with_report does
     return rc;
 }
+int llg_minimize(llg_solver* s, const llg_params* p, int32_t fmask, const llg_minimize_settings* st,
+                 llg_minimize_report* rep) {
+    int rc = bind(s);
+    if (!rc && (!p || !st || !rep)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc : s->eng->minimize(p, fmask, st, rep);
+}
+void llg_default_minimize_settings(llg_minimize_settings* st) {
+    std::memset(st, 0, sizeof(*st));
+    st->torque_threshold = 5e-4;
+    st->max_iters = 20000;
+    st->lambda0 = 2e-2;
+    st->lambda_min = 1e-5;
+    st->lambda_max = 5e-2;
+    st->grow = 1.05;
+    st->shrink = 0.8;
+    st->stall_iters = 5000;
+    st->stall_rel = 5e-4;
+    st->min_iters_before_stall = 500;
+    st->has_dm_stop = 1;
+    st->dm_stop = 1e-6;
+    st->dm_samples = 10;
+    st->has_dm_torque_gate = 1;
+    st->dm_torque_gate = 2e-3;
+    st->has_dm_torque_gate_max = 1;
+    st->dm_torque_gate_max = 5e-3;
+    st->dm_min_iters = 50;
+}
 void llg_default_relax_settings(llg_relax_settings* st) {
     std::memset(st, 0, sizeof(*st));
     st->max_err = 1e-5;
@@ -1592,6 +1724,12 @@ int llg_batch_relax(llg_batch* b, llg_params* params, int32_t fmask, const llg_r
     int rc = bind(b);
     if (!rc && (!params || !settings || !reports)) rc = set_error(LLG_ERR_INVALID, "null argument");
     return rc ? rc : b->eng->relax(params, fmask, settings, reports);
+}
+int llg_batch_minimize(llg_batch* b, const llg_params* params, int32_t fmask, const llg_minimize_settings* settings,
+                       llg_minimize_report* reports) {
+    int rc = bind(b);
+    if (!rc && (!params || !settings || !reports)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc : b->eng->minimize(params, fmask, settings, reports);
 }
 int llg_batch_compute_energy(llg_batch* b, const double* b_ext, llg_energy_breakdown* out) {
     int rc = bind(b);

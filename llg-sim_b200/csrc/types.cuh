@@ -27,10 +27,12 @@ struct FftPlan {
 enum MBuf : int { MB_M0 = 0, MB_M7 = 1, MB_S0 = 2, MB_S1 = 3 };
 enum KBuf : int { KB_NONE = 0, KB_K1 = 1, KB_K2, KB_K3, KB_K4, KB_K5, KB_K6, KB_K7 = 7 };
 
-enum RhsMode : int { RHS_LLG = 0, RHS_RELAX = 1, RHS_FIELD = 2, RHS_ENERGY = 3, RHS_TORQUE = 4 };
+// RHS_MINIMIZE: one damping-only descent update m' = normalize(m + lambda (m x B) x m)
+// written to the other parity buffer (minimize.rs:216-256)
+enum RhsMode : int { RHS_LLG = 0, RHS_RELAX = 1, RHS_FIELD = 2, RHS_ENERGY = 3, RHS_TORQUE = 4, RHS_MINIMIZE = 5 };
 enum ErrMode : int { ERR_NONE = 0, ERR_RK45 = 1, ERR_RK23 = 2 };
-// Requests of the device-side relax controller.
-enum ReqKind : int { REQ_NONE = 0, REQ_ENERGY = 1, REQ_TORQUE = 2, REQ_STEP = 3 };
+// Requests of the device-side relax and minimiser controllers.
+enum ReqKind : int { REQ_NONE = 0, REQ_ENERGY = 1, REQ_TORQUE = 2, REQ_STEP = 3, REQ_MINIMIZE = 4 };
 
 // Slots of the per-block FP64 partial reductions.
 enum RedSlot : int {
@@ -57,6 +59,7 @@ struct StepState {
     int err_code;
     int order;                    // 5 for RK45, 3 for RK23 (controller exponent 1/order)
     int req;                      // request of the device relax controller (ReqKind)
+    double lam;                   // minimiser pseudo-step lambda of the next update
     double red[RED_NSLOT];        // finalised reductions of the last reduction pass
 };
 

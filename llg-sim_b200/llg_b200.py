@@ -75,6 +75,11 @@ class RelaxSettings(C.Structure):
                 setattr(s, k, v)
         return s
 
+    def copy(self):
+        c = RelaxSettings()
+        C.memmove(C.byref(c), C.byref(self), C.sizeof(self))
+        return c
+
 
 class RelaxReport(C.Structure):
     _fields_ = [("accepted_steps", C.c_int64), ("rejected_steps", C.c_int64), ("torque_checks", C.c_int64),
@@ -82,6 +87,42 @@ class RelaxReport(C.Structure):
                 ("has_final_torque", C.c_int32), ("has_final_torque_max", C.c_int32),
                 ("final_torque", C.c_double), ("final_torque_max", C.c_double),
                 ("final_max_err", C.c_double), ("final_dt", C.c_double)]
+
+
+class MinimizeSettings(C.Structure):
+    """MinimizeSettings (minimize.rs:20-63); defaults from impl Default (minimize.rs:65-92).
+    The Option fields dm_stop / dm_torque_gate / dm_torque_gate_max take None in default()."""
+    _fields_ = [("torque_threshold", C.c_double), ("max_iters", C.c_int64), ("lambda0", C.c_double),
+                ("lambda_min", C.c_double), ("lambda_max", C.c_double), ("grow", C.c_double), ("shrink", C.c_double),
+                ("stall_iters", C.c_int64), ("stall_rel", C.c_double), ("min_iters_before_stall", C.c_int64),
+                ("has_dm_stop", C.c_int32), ("has_dm_torque_gate", C.c_int32),
+                ("has_dm_torque_gate_max", C.c_int32), ("reserved", C.c_int32), ("dm_stop", C.c_double),
+                ("dm_samples", C.c_int64), ("dm_torque_gate", C.c_double), ("dm_torque_gate_max", C.c_double),
+                ("dm_min_iters", C.c_int64)]
+
+    @classmethod
+    def default(cls, **kw):
+        s = cls()
+        lib().llg_default_minimize_settings(C.byref(s))
+        for k, v in kw.items():
+            if k in ("dm_stop", "dm_torque_gate", "dm_torque_gate_max"):
+                setattr(s, "has_" + k, 0 if v is None else 1)
+                setattr(s, k, 0.0 if v is None else float(v))
+            else:
+                setattr(s, k, v)
+        return s
+
+    def copy(self):
+        c = MinimizeSettings()
+        C.memmove(C.byref(c), C.byref(self), C.sizeof(self))
+        return c
+
+
+class MinimizeReport(C.Structure):
+    """MinimizeReport (minimize.rs:94-104)."""
+    _fields_ = [("iters", C.c_int64), ("converged", C.c_int32), ("stalled", C.c_int32),
+                ("dm_converged", C.c_int32), ("reserved", C.c_int32), ("final_torque", C.c_double),
+                ("final_max_dm", C.c_double), ("final_tmean", C.c_double), ("final_lambda", C.c_double)]
 
 
 class EnergyBreakdown(C.Structure):
@@ -130,6 +171,9 @@ def lib():
                                        i64, C.c_double, i64, P(i64), P(i64), dp]),
             "llg_relax": (C.c_int, [vp, P(_Params), i32, P(RelaxSettings), P(RelaxReport)]),
             "llg_default_relax_settings": (None, [P(RelaxSettings)]),
+            "llg_minimize": (C.c_int, [vp, P(_Params), i32, P(MinimizeSettings), P(MinimizeReport)]),
+            "llg_default_minimize_settings": (None, [P(MinimizeSettings)]),
+            "llg_batch_minimize": (C.c_int, [vp, P(_Params), i32, P(MinimizeSettings), P(MinimizeReport)]),
             "llg_compute_energy": (C.c_int, [vp, dp, P(EnergyBreakdown)]),
             "llg_torque_metric": (C.c_int, [vp, P(_Params), i32, i32, dp]),
             "llg_demag_kernel_kspace": (C.c_int, [vp, dp]),
@@ -345,6 +389,13 @@ class Solver:
         params.dt = p.dt
         return rep
 
+    def minimize(self, params, field_mask, settings):
+        """minimize_damping_only (minimize.rs:107): the resident state is updated in place."""
+        p = params._c()
+        rep = MinimizeReport()
+        _check(lib().llg_minimize(self.h, C.byref(p), int(field_mask), C.byref(settings), C.byref(rep)))
+        return rep
+
     def compute_energy(self, b_ext):
         be = np.ascontiguousarray(np.asarray(b_ext, dtype=np.float64).reshape(3))
         e = EnergyBreakdown()
@@ -462,6 +513,13 @@ class Batch:
         _check(lib().llg_batch_relax(self.h, P, int(field_mask), C.byref(settings), reps))
         for i, p in enumerate(params):
             p.dt = P[i].dt
+        return list(reps)
+
+    def minimize(self, params, field_mask, settings):
+        """minimize_damping_only (minimize.rs:107) for every film; one report per film."""
+        P = self._params(params)
+        reps = (MinimizeReport * self.n)()
+        _check(lib().llg_batch_minimize(self.h, P, int(field_mask), C.byref(settings), reps))
         return list(reps)
 
     def warm_start(self, net, b_exts):

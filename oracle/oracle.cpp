@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <memory>
 #include <vector>
 
@@ -1141,6 +1142,278 @@ void orc_relax(orc_solver* s, double* m, orc_params* p, int fmask, orc_relax_set
         }
     }
     finish(2);
+}
+
+void orc_default_minimize_settings(orc_minimize_settings* st) {
+    // impl Default for MinimizeSettings, minimize.rs:65-92
+    std::memset(st, 0, sizeof(*st));
+    st->torque_threshold = 5e-4;
+    st->max_iters = 20000;
+    st->lambda0 = 2e-2;
+    st->lambda_min = 1e-5;
+    st->lambda_max = 5e-2;
+    st->grow = 1.05;
+    st->shrink = 0.8;
+    st->stall_iters = 5000;
+    st->stall_rel = 5e-4;
+    st->min_iters_before_stall = 500;
+    st->has_dm_stop = 1;
+    st->dm_stop = 1e-6;
+    st->dm_samples = 10;
+    st->has_dm_torque_gate = 1;
+    st->dm_torque_gate = 2e-3;
+    st->has_dm_torque_gate_max = 1;
+    st->dm_torque_gate_max = 5e-3;
+    st->dm_min_iters = 50;
+}
+
+void orc_minimize(orc_solver* s, double* m, const orc_params* p, int fmask, const orc_minimize_settings* st,
+                  orc_minimize_report* rep) {
+    // minimize_damping_only, minimize.rs:107-369 (the sequential per-cell pass, :216-256)
+    const int64_t n = s->n;
+    std::vector<double> b(n * 3);
+    double lambda = st->lambda0;
+    double t_prev_mean = INFINITY;
+    int64_t stall_count = 0;
+    std::deque<double> dm_hist;
+    double last_max_dm = INFINITY, last_tmax = INFINITY, last_tmean = INFINITY;
+    const size_t samples = (size_t)std::max<int64_t>(st->dm_samples, 1);
+    auto report = [&](int64_t iters, double ft, bool conv, bool stalled, double mdm, bool dmc, double tm) {
+        rep->iters = iters;
+        rep->converged = conv ? 1 : 0;
+        rep->stalled = stalled ? 1 : 0;
+        rep->dm_converged = dmc ? 1 : 0;
+        rep->final_torque = ft;
+        rep->final_max_dm = mdm;
+        rep->final_tmean = tm;
+        rep->final_lambda = lambda;
+    };
+    for (int64_t it = 0; it < st->max_iters; ++it) {
+        build_h_eff(s, m, p->b_ext, fmask, b.data());
+        double tmax = 0.0, tsum = 0.0, max_dm = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            const double* m0 = &m[i * 3];
+            double t[3], d[3];
+            vcross(m0, &b[i * 3], t);
+            const double tmag = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+            tsum += tmag;
+            if (tmag > tmax) tmax = tmag;
+            vcross(t, m0, d);  // damping-only direction (m x B) x m
+            double x = m0[0] + lambda * d[0];
+            double y = m0[1] + lambda * d[1];
+            double z = m0[2] + lambda * d[2];
+            const double n2 = x * x + y * y + z * z;
+            if (n2 > 0.0) {
+                const double inv = 1.0 / std::sqrt(n2);
+                x *= inv;
+                y *= inv;
+                z *= inv;
+            }
+            const double ddx = x - m0[0], ddy = y - m0[1], ddz = z - m0[2];
+            const double dm = std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+            if (dm > max_dm) max_dm = dm;
+            m[i * 3] = x;
+            m[i * 3 + 1] = y;
+            m[i * 3 + 2] = z;
+        }
+        const double tmean = tsum / std::max((double)n, 1.0);
+        last_tmean = tmean;
+        if (tmax < st->torque_threshold) {
+            report(it + 1, tmax, true, false, max_dm, false, tmean);
+            return;
+        }
+        last_max_dm = max_dm;
+        last_tmax = tmax;
+        if (st->has_dm_stop && it + 1 >= st->dm_min_iters) {
+            dm_hist.push_back(max_dm);
+            while (dm_hist.size() > samples) dm_hist.pop_front();
+            bool all = dm_hist.size() == samples;
+            for (double v : dm_hist) all = all && v < st->dm_stop;
+            if (all) {
+                const bool mean_ok = !st->has_dm_torque_gate || tmean <= st->dm_torque_gate;
+                const bool max_ok = !st->has_dm_torque_gate_max || tmax <= st->dm_torque_gate_max;
+                report(it + 1, tmax, mean_ok && max_ok, false, max_dm, true, tmean);
+                return;
+            }
+        }
+        if (tmean < t_prev_mean) lambda = std::fmin(lambda * st->grow, st->lambda_max);
+        else lambda = std::fmax(lambda * st->shrink, st->lambda_min);
+        if (it + 1 >= st->min_iters_before_stall && std::isfinite(t_prev_mean)) {
+            const double good = t_prev_mean - tmean;
+            const double need = st->stall_rel * std::fmax(std::fabs(t_prev_mean), 1e-30);
+            if (good <= need) stall_count += 1;
+            else stall_count = 0;
+        }
+        if (stall_count >= st->stall_iters) {
+            report(it + 1, tmax, false, true, last_max_dm, false, tmean);
+            return;
+        }
+        t_prev_mean = tmean;
+    }
+    report(std::max<int64_t>(st->max_iters, 0), last_tmax, false, false, last_max_dm, false, last_tmean);
+}
+
+// ---------------------------------------------------------------------------------------------
+// AMR consumers of the uniform FFT demag
+
+int64_t orc_validated_ratio(int64_t nx, int64_t ny, int64_t ratio) {
+    // validated_ratio, coarse_fft_demag.rs:118-150 (warnings omitted)
+    if (ratio <= 1) return 1;
+    if (nx % ratio != 0 || ny % ratio != 0) return 1;
+    if (nx / ratio < 4 || ny / ratio < 4) return 1;
+    return ratio;
+}
+
+static inline int64_t clamp_idx(int64_t i, int64_t n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
+
+void orc_sample_bilinear(const orc_grid* g, const double* f, double x, double y, double out[3]) {
+    // sample_bilinear, amr/interp.rs:28-72
+    const int64_t nx = g->nx, ny = g->ny;
+    if (nx == 0 || ny == 0) {
+        out[0] = out[1] = out[2] = 0.0;
+        return;
+    }
+    const double fx = x / g->dx - 0.5, fy = y / g->dy - 0.5;
+    const double i0f = std::floor(fx), j0f = std::floor(fy);
+    const double tx = fx - i0f, ty = fy - j0f;
+    const int64_t i0 = clamp_idx((int64_t)i0f, nx), j0 = clamp_idx((int64_t)j0f, ny);
+    const int64_t i1 = clamp_idx((int64_t)i0f + 1, nx), j1 = clamp_idx((int64_t)j0f + 1, ny);
+    const double* v00 = &f[(j0 * nx + i0) * 3];
+    const double* v10 = &f[(j0 * nx + i1) * 3];
+    const double* v01 = &f[(j1 * nx + i0) * 3];
+    const double* v11 = &f[(j1 * nx + i1) * 3];
+    for (int c = 0; c < 3; ++c) {
+        const double a = v00[c] * (1.0 - tx) + v10[c] * tx;
+        const double b = v01[c] * (1.0 - tx) + v11[c] * tx;
+        out[c] = a * (1.0 - ty) + b * ty;
+    }
+}
+
+void orc_restrict_m_to_coarse(const orc_grid* base, const double* m_coarse, int32_t n_patches,
+                              const orc_amr_patch* patches, double* out) {
+    // restrict_m_to_coarse, coarse_fft_demag.rs:170-240: un-normalised area average of each
+    // patch's material fine cells, patches in order (finer levels last overwrite)
+    const int64_t n = base->nx * base->ny;
+    std::memcpy(out, m_coarse, sizeof(double) * 3 * (size_t)n);
+    for (int q = 0; q < n_patches; ++q) {
+        const orc_amr_patch& p = patches[q];
+        const int64_t r = p.ratio, gh = p.ghost, pnx = p.cnx * r + 2 * gh;
+        for (int64_t jc = 0; jc < p.cny; ++jc)
+            for (int64_t ic = 0; ic < p.cnx; ++ic) {
+                double* dst = &out[((p.j0 + jc) * base->nx + p.i0 + ic) * 3];
+                if (p.parent_material && !p.parent_material[jc * p.cnx + ic]) {
+                    dst[0] = dst[1] = dst[2] = 0.0;
+                    continue;
+                }
+                double sum[3] = {0.0, 0.0, 0.0};
+                int64_t n_mat = 0;
+                for (int64_t fj = 0; fj < r; ++fj)
+                    for (int64_t fi = 0; fi < r; ++fi) {
+                        const int64_t idx = (gh + jc * r + fj) * pnx + gh + ic * r + fi;
+                        if (p.geom_mask_fine && !p.geom_mask_fine[idx]) continue;
+                        sum[0] += p.m[idx * 3];
+                        sum[1] += p.m[idx * 3 + 1];
+                        sum[2] += p.m[idx * 3 + 2];
+                        n_mat += 1;
+                    }
+                if (n_mat == 0) {
+                    dst[0] = dst[1] = dst[2] = 0.0;
+                } else {
+                    const double inv = 1.0 / (double)n_mat;
+                    dst[0] = sum[0] * inv;
+                    dst[1] = sum[1] * inv;
+                    dst[2] = sum[2] * inv;
+                }
+            }
+    }
+}
+
+void orc_restrict_l0_to_demag_grid(int64_t nx_l0, const double* l0_m, int64_t dnx, int64_t dny, int64_t ratio,
+                                   double* out) {
+    // restrict_l0_to_demag_grid, coarse_fft_demag.rs:256-290
+    const double inv_r2 = 1.0 / (double)(ratio * ratio);
+    for (int64_t jd = 0; jd < dny; ++jd)
+        for (int64_t id = 0; id < dnx; ++id) {
+            double sum[3] = {0.0, 0.0, 0.0};
+            for (int64_t fj = 0; fj < ratio; ++fj) {
+                const int64_t row = (jd * ratio + fj) * nx_l0 + id * ratio;
+                for (int64_t fi = 0; fi < ratio; ++fi)
+                    for (int c = 0; c < 3; ++c) sum[c] += l0_m[(row + fi) * 3 + c];
+            }
+            for (int c = 0; c < 3; ++c) out[(jd * dnx + id) * 3 + c] = sum[c] * inv_r2;
+        }
+}
+
+static void uniform_demag(const orc_grid* g, const orc_material* mat, const double* m, double* b) {
+    // compute_demag_field (demag_fft_uniform.rs:146-186): zero, then add unless !mat.demag
+    orc_solver* s = orc_solver_create(g, mat, nullptr);
+    orc_demag_field(s, m, b);
+    orc_solver_destroy(s);
+}
+
+void orc_coarse_fft_demag(const orc_grid* base, const orc_material* mat, const double* m_coarse,
+                          int32_t n_patches, const orc_amr_patch* patches, int64_t ratio, double* b_coarse,
+                          double* b_patches) {
+    // compute_coarse_fft_demag, coarse_fft_demag.rs:367-511
+    const int64_t n = base->nx * base->ny;
+    if (!mat->demag) {
+        std::fill(b_coarse, b_coarse + 3 * n, 0.0);
+        return;   // no patch fields (empty vectors in the reference)
+    }
+    // a ratio that is not a power of two falls back to 1 as demag_coarsen_ratio does (:98-106)
+    const bool pow2 = ratio >= 1 && (ratio & (ratio - 1)) == 0;
+    const int64_t r = pow2 ? orc_validated_ratio(base->nx, base->ny, ratio) : 1;
+    std::vector<double> enhanced(3 * n);
+    orc_restrict_m_to_coarse(base, m_coarse, n_patches, patches, enhanced.data());
+    if (r <= 1) {
+        uniform_demag(base, mat, enhanced.data(), b_coarse);
+    } else {
+        const orc_grid dg = {base->nx / r, base->ny / r, base->dx * (double)r, base->dy * (double)r, base->dz};
+        std::vector<double> dm(3 * dg.nx * dg.ny), db(3 * dg.nx * dg.ny);
+        orc_restrict_l0_to_demag_grid(base->nx, enhanced.data(), dg.nx, dg.ny, r, dm.data());
+        uniform_demag(&dg, mat, dm.data(), db.data());
+        // interpolate_demag_to_l0 (:299-318)
+        for (int64_t j = 0; j < base->ny; ++j) {
+            const double y = ((double)j + 0.5) * base->dy;
+            for (int64_t i = 0; i < base->nx; ++i) {
+                const double x = ((double)i + 0.5) * base->dx;
+                orc_sample_bilinear(&dg, db.data(), x, y, &b_coarse[(j * base->nx + i) * 3]);
+            }
+        }
+    }
+    // sample_demag_to_patch (:327-340) for every patch, incl. ghosts
+    double* dst = b_patches;
+    for (int q = 0; q < n_patches; ++q) {
+        const orc_amr_patch& p = patches[q];
+        const int64_t pnx = p.cnx * p.ratio + 2 * p.ghost, pny = p.cny * p.ratio + 2 * p.ghost;
+        const double fdx = base->dx / (double)p.ratio, fdy = base->dy / (double)p.ratio;
+        const double gi0 = (double)(p.i0 * p.ratio), gj0 = (double)(p.j0 * p.ratio);
+        for (int64_t j = 0; j < pny; ++j)
+            for (int64_t i = 0; i < pnx; ++i) {
+                // Patch2D::cell_center_xy, amr/patch.rs:377-387
+                const double li = (double)i - (double)p.ghost, lj = (double)j - (double)p.ghost;
+                const double x = (gi0 + li + 0.5) * fdx, y = (gj0 + lj + 0.5) * fdy;
+                orc_sample_bilinear(base, b_coarse, x, y, dst);
+                dst += 3;
+            }
+    }
+}
+
+void orc_allfft_demag(const orc_grid* fine, const orc_material* mat, const double* m_fine, const uint8_t* fine_mask,
+                      const orc_grid* base, double* b_fine, double* b_coarse) {
+    // AmrDemagMode::AllFft, amr/stepper.rs:799-835
+    const int64_t nf = fine->nx * fine->ny;
+    uniform_demag(fine, mat, m_fine, b_fine);
+    if (fine_mask)
+        for (int64_t i = 0; i < nf; ++i)
+            if (!fine_mask[i]) b_fine[3 * i] = b_fine[3 * i + 1] = b_fine[3 * i + 2] = 0.0;
+    for (int64_t j = 0; j < base->ny; ++j) {
+        const double y = ((double)j + 0.5) * base->dy;
+        for (int64_t i = 0; i < base->nx; ++i) {
+            const double x = ((double)i + 0.5) * base->dx;
+            orc_sample_bilinear(fine, b_fine, x, y, &b_coarse[(j * base->nx + i) * 3]);
+        }
+    }
 }
 
 void orc_kernel_components(double dx, double dy, double dz, int64_t sx, int64_t sy, double accuracy,

@@ -78,6 +78,30 @@ typedef struct orc_relax_report {
     double final_torque, final_torque_max, final_max_err, final_dt;
 } orc_relax_report;
 
+/* MinimizeSettings (minimize.rs:20-63); Option<f64> fields as has_* flags.
+ * `parallel` and `print_every` change neither the result nor the report and are
+ * not carried. */
+typedef struct orc_minimize_settings {
+    double torque_threshold;
+    int64_t max_iters;
+    double lambda0, lambda_min, lambda_max, grow, shrink;
+    int64_t stall_iters;
+    double stall_rel;
+    int64_t min_iters_before_stall;
+    int32_t has_dm_stop, has_dm_torque_gate, has_dm_torque_gate_max, reserved;
+    double dm_stop;
+    int64_t dm_samples;
+    double dm_torque_gate, dm_torque_gate_max;
+    int64_t dm_min_iters;
+} orc_minimize_settings;
+
+/* MinimizeReport (minimize.rs:94-104) */
+typedef struct orc_minimize_report {
+    int64_t iters;
+    int32_t converged, stalled, dm_converged, reserved;
+    double final_torque, final_max_dm, final_tmean, final_lambda;
+} orc_minimize_report;
+
 typedef struct orc_energy {
     double exchange, anisotropy, zeeman, dmi, demag;
 } orc_energy;
@@ -103,6 +127,38 @@ void orc_step_rk23_relax(orc_solver* s, double* m, orc_params* p, int field_mask
 void orc_relax(orc_solver* s, double* m, orc_params* p, int field_mask, orc_relax_settings* st,
                orc_relax_report* rep);
 void orc_default_relax_settings(orc_relax_settings* st);
+void orc_default_minimize_settings(orc_minimize_settings* st);
+void orc_minimize(orc_solver* s, double* m, const orc_params* p, int field_mask, const orc_minimize_settings* st,
+                  orc_minimize_report* rep);
+/* ---- AMR consumers of the uniform FFT demag (coarse_fft_demag.rs, amr/stepper.rs) ---- */
+/* Patch2D (amr/patch.rs:15-80) as the demag consumers read it: coarse_rect in
+ * base-grid cells, refinement ratio relative to the base grid, ghost width; m on
+ * the patch grid incl. ghosts ((cny*ratio+2*ghost) x (cnx*ratio+2*ghost), AoS);
+ * geom_mask_fine on the same grid (NULL: none); parent_material[cny*cnx]
+ * (NULL: all material). */
+typedef struct orc_amr_patch {
+    int64_t i0, j0, cnx, cny, ratio, ghost;
+    const double* m;
+    const uint8_t* geom_mask_fine;
+    const uint8_t* parent_material;
+} orc_amr_patch;
+
+int64_t orc_validated_ratio(int64_t nx, int64_t ny, int64_t ratio);
+void orc_sample_bilinear(const orc_grid* g, const double* field, double x, double y, double out[3]);
+void orc_restrict_m_to_coarse(const orc_grid* base, const double* m_coarse, int32_t n_patches,
+                              const orc_amr_patch* patches, double* out);
+void orc_restrict_l0_to_demag_grid(int64_t nx_l0, const double* l0_m, int64_t dnx, int64_t dny, int64_t ratio,
+                                   double* out);
+/* compute_coarse_fft_demag (coarse_fft_demag.rs:367-511) with an explicit
+ * coarsening ratio (validated as the reference validates its environment value);
+ * b_patches receives every patch's full grid, patches concatenated in order. */
+void orc_coarse_fft_demag(const orc_grid* base, const orc_material* mat, const double* m_coarse,
+                          int32_t n_patches, const orc_amr_patch* patches, int64_t ratio, double* b_coarse,
+                          double* b_patches);
+/* The AllFft branch of AmrStepper::compute_demag (amr/stepper.rs:799-835). */
+void orc_allfft_demag(const orc_grid* fine, const orc_material* mat, const double* m_fine, const uint8_t* fine_mask,
+                      const orc_grid* base, double* b_fine, double* b_coarse);
+
 void orc_energy_breakdown(orc_solver* s, const double* m, const double b_ext[3], orc_energy* out);
 double orc_torque_metric(int64_t n, const double* m, const double* b, int metric);
 

@@ -47,6 +47,22 @@ class RelaxReport(C.Structure):
                 ("final_max_err", C.c_double), ("final_dt", C.c_double)]
 
 
+class MinimizeSettings(C.Structure):
+    _fields_ = [("torque_threshold", C.c_double), ("max_iters", C.c_int64), ("lambda0", C.c_double),
+                ("lambda_min", C.c_double), ("lambda_max", C.c_double), ("grow", C.c_double), ("shrink", C.c_double),
+                ("stall_iters", C.c_int64), ("stall_rel", C.c_double), ("min_iters_before_stall", C.c_int64),
+                ("has_dm_stop", C.c_int32), ("has_dm_torque_gate", C.c_int32),
+                ("has_dm_torque_gate_max", C.c_int32), ("reserved", C.c_int32), ("dm_stop", C.c_double),
+                ("dm_samples", C.c_int64), ("dm_torque_gate", C.c_double), ("dm_torque_gate_max", C.c_double),
+                ("dm_min_iters", C.c_int64)]
+
+
+class MinimizeReport(C.Structure):
+    _fields_ = [("iters", C.c_int64), ("converged", C.c_int32), ("stalled", C.c_int32),
+                ("dm_converged", C.c_int32), ("reserved", C.c_int32), ("final_torque", C.c_double),
+                ("final_max_dm", C.c_double), ("final_tmean", C.c_double), ("final_lambda", C.c_double)]
+
+
 class Energy(C.Structure):
     _fields_ = [("exchange", C.c_double), ("anisotropy", C.c_double), ("zeeman", C.c_double),
                 ("dmi", C.c_double), ("demag", C.c_double)]
@@ -80,6 +96,9 @@ def lib():
         L.orc_relax.argtypes = [vp, dp, C.POINTER(Params), C.c_int, C.POINTER(RelaxSettings),
                                 C.POINTER(RelaxReport)]
         L.orc_default_relax_settings.argtypes = [C.POINTER(RelaxSettings)]
+        L.orc_minimize.argtypes = [vp, dp, C.POINTER(Params), C.c_int, C.POINTER(MinimizeSettings),
+                                   C.POINTER(MinimizeReport)]
+        L.orc_default_minimize_settings.argtypes = [C.POINTER(MinimizeSettings)]
         L.orc_energy_breakdown.argtypes = [vp, dp, dp, C.POINTER(Energy)]
         L.orc_torque_metric.restype = C.c_double
         L.orc_torque_metric.argtypes = [C.c_int64, dp, dp, C.c_int]
@@ -143,6 +162,20 @@ def default_relax_settings(**kw):
             else:
                 s.has_torque_threshold = 1
                 s.torque_threshold = float(v)
+        else:
+            setattr(s, k, v)
+    return s
+
+
+def default_minimize_settings(**kw):
+    """MinimizeSettings::default() (minimize.rs:65-92) with keyword overrides; the
+    Option fields dm_stop / dm_torque_gate / dm_torque_gate_max take None."""
+    s = MinimizeSettings()
+    lib().orc_default_minimize_settings(C.byref(s))
+    for k, v in kw.items():
+        if k in ("dm_stop", "dm_torque_gate", "dm_torque_gate_max"):
+            setattr(s, "has_" + k, 0 if v is None else 1)
+            setattr(s, k, 0.0 if v is None else float(v))
         else:
             setattr(s, k, v)
     return s
@@ -215,6 +248,13 @@ class Solver:
         assert m.dtype == np.float64 and m.flags.c_contiguous
         rep = RelaxReport()
         lib().orc_relax(self.h, _dp(m), C.byref(params), int(field_mask), C.byref(settings), C.byref(rep))
+        return rep
+
+    def minimize(self, m, params, field_mask, settings):
+        """minimize_damping_only (minimize.rs:107), in place on m (float64 [n,3])."""
+        assert m.dtype == np.float64 and m.flags.c_contiguous
+        rep = MinimizeReport()
+        lib().orc_minimize(self.h, _dp(m), C.byref(params), int(field_mask), C.byref(settings), C.byref(rep))
         return rep
 
     def energy(self, m, b_ext):

@@ -42,6 +42,17 @@ def test_default_relax_settings_match_oracle(gpu, orc):
         assert getattr(a, name) == getattr(b, name), name
 
 
+def test_default_minimize_settings_match_oracle(gpu, orc):
+    a = gpu.MinimizeSettings.default()
+    b = orc.default_minimize_settings()
+    for name, _ in gpu.MinimizeSettings._fields_:
+        assert getattr(a, name) == getattr(b, name), name
+    # MinimizeSettings::default (minimize.rs:65-92)
+    assert (a.torque_threshold, a.max_iters, a.lambda0, a.dm_stop, a.dm_samples) == (5e-4, 20000, 2e-2, 1e-6, 10)
+    assert a.has_dm_stop and a.has_dm_torque_gate and a.has_dm_torque_gate_max
+    assert C.sizeof(gpu.MinimizeSettings) == 136 and C.sizeof(gpu.MinimizeReport) == 56
+
+
 def test_warmstart_param_count_matches_reference_layout(gpu):
     import warmstart_ref
 
