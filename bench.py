@@ -335,6 +335,72 @@ def warmstart_leg(L, torch, stream, max_over_ranks, n_films=16, size=256):
     return out
 
 
+def amr_leg(L, reps=5):
+    """The AMR consumers of the uniform FFT demag through the public API (host arrays in
+    and out, wall clock per call after a warm-up call): compute_coarse_fft_demag on a
+    192x192 base film refined by 7 patches (ratio 2/4/8) and the AllFft demag of the
+    same film at 8x resolution (1536x1536, FP64 FFT of 3072x3072), the sizes
+    coarse_fft_demag.rs:28-31 quotes (all_fft ~29 s, coarse_fft 0.3-0.5 s + 0.1 s on
+    the reference's CPU).  The FP64 oracle times the coarse-FFT evaluation on the host
+    (operator cached, as the reference caches it)."""
+    import time
+    import workloads as W
+
+    nx = ny = 192
+    dx = dy = 4e-9
+    dz = 3e-9
+    ms = 8.0e5
+    mc, specs = W.amr_vortex_hierarchy(nx, ny, dx, dy, dz)
+    patches = [L.AmrPatch(p.i0, p.j0, p.cnx, p.cny, p.ratio, p.ghost, p.m) for p in specs]
+    mat = L.Material(ms, 1.3e-11, demag=True)
+    out = {"workload": "vortex, 192x192 base of 4x4x3 nm cells, Ms 8e5; patches: four 38x38 ratio 2, two 19x19 "
+                       "ratio 4, one 12x12 ratio 8 (ghost 2); AllFft on the 1536x1536 fine grid",
+           "patch_cells": int(sum(p.pnx * p.pny for p in patches))}
+    t0 = time.perf_counter()
+    h = L.AmrDemag(L.Grid2D(nx, ny, dx, dy, dz))
+    out["coarse_build_s"] = time.perf_counter() - t0
+    h.compute(mat, mc, patches)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        bc, bp = h.compute(mat, mc, patches)
+    out["coarse_fft_ms"] = (time.perf_counter() - t0) / reps * 1e3
+    h.close()
+    h2 = L.AmrDemag(L.Grid2D(nx, ny, dx, dy, dz), coarsen_ratio=2)
+    h2.compute(mat, mc, patches)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        h2.compute(mat, mc, patches)
+    out["coarse_fft_r2_ms"] = (time.perf_counter() - t0) / reps * 1e3
+    h2.close()
+    fg = L.Grid2D(8 * nx, 8 * ny, dx / 8, dy / 8, dz)
+    t0 = time.perf_counter()
+    op = L.DemagOp(fg)
+    out["allfft_build_s"] = time.perf_counter() - t0
+    mf = W.amr_fine_vortex(8 * nx, 8 * ny, dx / 8, dy / 8)
+    bg = L.Grid2D(nx, ny, dx, dy, dz)
+    L.allfft_demag(op, mat, mf, None, bg)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        L.allfft_demag(op, mat, mf, None, bg)
+    out["allfft_ms"] = (time.perf_counter() - t0) / reps * 1e3
+    out["allfft_io_bytes"] = int(mf.nbytes * 2 + nx * ny * 24)
+    op.close()
+    try:
+        import oracle as O
+
+        og = O.make_grid(nx, ny, dx, dy, dz)
+        om = O.make_material(ms, 1.3e-11, demag=True)
+        O.coarse_fft_demag(og, om, mc, specs)          # builds and caches the operator
+        t0 = time.perf_counter()
+        oc, _ = O.coarse_fft_demag(og, om, mc, specs)
+        out["cpu_coarse_fft_ms"] = (time.perf_counter() - t0) * 1e3
+        out["cpu_threads"] = O.get_threads()
+        out["coarse_max_rel_diff_vs_fp64_oracle"] = float(np.abs(bc - oc).max() / np.abs(oc).max())
+    except Exception as exc:   # the oracle library is optional on a GPU box
+        out["cpu_coarse_fft_ms"] = f"unavailable: {exc}"
+    return out
+
+
 def reduce_over_ranks(dist, x, op, device):
     """x reduced over the process group (op "max" or "sum"); x itself without one."""
     if dist is None:
@@ -510,6 +576,9 @@ def run_gpu(args):
     warm = None
     if not args.no_warmstart:
         warm = warmstart_leg(L, torch, stream, max_over_ranks)
+    amr = None
+    if not args.no_amr and world == 1:
+        amr = amr_leg(L)
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -525,7 +594,8 @@ def run_gpu(args):
                            "l2": "inputs larger than L2: ~190 MB per film working set (m, 7 torques, stage states, "
                                  "25 MB spectrum, 16 MB kernel) vs 126 MB L2"},
                 "clocks": clk, "gpu_launches": launches, "roofline": roofline, "roofline_step": roofline_step,
-                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "warm_start": warm, "cpu_baseline": cpu}
+                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "warm_start": warm, "amr_demag": amr,
+                "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     s.close()
     if dist is not None:
@@ -548,6 +618,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-flow", action="store_true")
     ap.add_argument("--no-warmstart", action="store_true")
+    ap.add_argument("--no-amr", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -316,6 +316,49 @@ int llg_demag_cache_filename(const llg_grid* grid, int64_t pbc_x, int64_t pbc_y,
  * with (cin, cout) = (7,32), (32,32) x4, (32,3); llg_warmstart_param_count()
  * gives the total.
  * ------------------------------------------------------------------------- */
+/* ---------------- AMR consumers of the uniform FFT demag ----------------
+ * Patch2D (amr/patch.rs:15-80) as the demag consumers read it: coarse_rect
+ * (i0, j0, cnx, cny) in base-grid cells, refinement ratio relative to the base
+ * grid, ghost width; m on the patch grid incl. ghosts, AoS FP64
+ * [(cny*ratio + 2*ghost) * (cnx*ratio + 2*ghost)][3]; geom_mask_fine on the same
+ * grid (NULL: none); parent_material[cny*cnx] (NULL: all material).  Patch lists
+ * are in the reference's processing order (level 1, then level 2, ...), later
+ * patches overwriting earlier ones. */
+typedef struct llg_amr_patch {
+    int64_t i0, j0, cnx, cny, ratio, ghost;
+    const double* m;
+    const uint8_t* geom_mask_fine;
+    const uint8_t* parent_material;
+} llg_amr_patch;
+typedef struct llg_amr_demag llg_amr_demag;
+/* validated_ratio (coarse_fft_demag.rs:118-150) */
+int64_t llg_amr_validated_ratio(int64_t nx, int64_t ny, int64_t ratio);
+/* cells of a patch grid including ghosts */
+int64_t llg_amr_patch_cells(const llg_amr_patch* p);
+/* Coarse-FFT demag context for a base (L0) grid: the FFT demag operator of the
+ * base grid, or with coarsen_ratio R > 1 of the (nx/R) x (ny/R) demag grid with
+ * R dx x R dy cells.  R follows LLG_DEMAG_COARSEN_RATIO's rules: not a power of
+ * two, not dividing nx and ny, or leaving fewer than 4 cells -> 1 (read back with
+ * llg_amr_demag_ratio). */
+int llg_amr_demag_create(llg_ctx* ctx, const llg_grid* base, int64_t coarsen_ratio, llg_amr_demag** out);
+int llg_amr_demag_ratio(const llg_amr_demag* h, int64_t* ratio);
+int llg_amr_demag_destroy(llg_amr_demag* h);
+/* restrict_m_to_coarse (coarse_fft_demag.rs:170-240): un-normalised area averages
+ * of the patches over L0 (AoS FP64 base grid in and out). */
+int llg_amr_restrict_m(llg_amr_demag* h, const double* m_coarse, int32_t n_patches, const llg_amr_patch* patches,
+                       double* out);
+/* compute_coarse_fft_demag (coarse_fft_demag.rs:367-511).  b_coarse: base grid AoS;
+ * b_patches: every patch's grid incl. ghosts, concatenated in list order
+ * (sum of llg_amr_patch_cells x 3 doubles).  Without Material::demag b_coarse is
+ * zeroed and b_patches is not written (the reference returns no patch fields). */
+int llg_coarse_fft_demag(llg_amr_demag* h, const llg_material* mat, const double* m_coarse, int32_t n_patches,
+                         const llg_amr_patch* patches, double* b_coarse, double* b_patches);
+/* The AllFft branch of AmrStepper::compute_demag (amr/stepper.rs:799-835): demag of
+ * the flattened fine grid (fine_op: llg_demag_op_create with pbc 0, 0), zero where
+ * fine_mask is 0 (NULL: no mask), bilinear samples at the base-grid cell centres. */
+int llg_amr_allfft_demag(llg_demag_op* fine_op, const llg_material* mat, const double* m_fine,
+                         const uint8_t* fine_mask, const llg_grid* base, double* b_fine, double* b_coarse);
+
 typedef struct llg_warmstart llg_warmstart;
 int64_t llg_warmstart_param_count(void);
 int llg_warmstart_create(llg_ctx* ctx, const float* params, int64_t n_params, llg_warmstart** out);

@@ -1,6 +1,7 @@
 // build_api.h — host-side entry points shared between the compilation units.
 #pragma once
 #include <cuda_runtime.h>
+#include "../../include/llg_b200.h"
 #include "types.cuh"
 
 // Sets the calling thread's message returned by llg_last_error().
@@ -24,6 +25,11 @@ cudaError_t build_demag_kernel_pbc(int nx, int ny, double dx, double dy, double 
 cudaError_t build_demag_kernel(int nx, int ny, double dx, double dy, double dz, bool fp64_out, void* khat_out,
                                double* k64_out_dev, cudaStream_t s);
 
+
+// The demag operator of llg_demag_op_create applied to a device AoS FP64 m on
+// stream s (the input is read before the output is written, so they may alias).
+int demag_op_apply_device(llg_demag_op* op, double ms, const double* d_m_aos, double* d_b_aos, cudaStream_t s);
+void demag_op_info(const llg_demag_op* op, int* device, llg_grid* g, int* pbc_x, int* pbc_y);
 
 // Launch geometry of one film set.
 struct LaunchGeom {

@@ -101,6 +101,40 @@ __global__ void k_pbc_extract(const cx<double>* __restrict__ M, int nx, int ny, 
     }
 }
 
+}  // namespace
+
+namespace llg {
+
+int demag_op_apply_device(llg_demag_op* op, double ms, const double* d_m_aos, double* d_b_aos, cudaStream_t s) {
+    const long long np = (long long)op->px * op->py;
+    k_pbc_pack<<<1184, 256, 0, s>>>(d_m_aos, op->nx, op->ny, op->px, op->py, ms, op->M);
+    PBC_TRY(cudaGetLastError());
+    PBC_TRY(llg::launch_fft_strided<double>(op->M, op->px, op->twx, 1, op->py, op->px, 3, np, false, s));
+    PBC_TRY(llg::launch_fft_strided<double>(op->M, op->py, op->twy, op->px, op->px, 1, 3, np, false, s));
+    k_pbc_multiply<<<1184, 256, 0, s>>>(op->K, np, op->M);
+    PBC_TRY(cudaGetLastError());
+    PBC_TRY(llg::launch_fft_strided<double>(op->M, op->px, op->twx, 1, op->py, op->px, 3, np, true, s));
+    PBC_TRY(llg::launch_fft_strided<double>(op->M, op->py, op->twy, op->px, op->px, 1, 3, np, true, s));
+    k_pbc_extract<<<1184, 256, 0, s>>>(op->M, op->nx, op->ny, op->px, op->py, 1.0 / (double)np, d_b_aos);
+    PBC_TRY(cudaGetLastError());
+    return LLG_OK;
+}
+
+void demag_op_info(const llg_demag_op* op, int* device, llg_grid* g, int* pbc_x, int* pbc_y) {
+    *device = op->device;
+    g->nx = op->nx;
+    g->ny = op->ny;
+    g->dx = op->dx;
+    g->dy = op->dy;
+    g->dz = op->dz;
+    *pbc_x = op->pbc_x;
+    *pbc_y = op->pbc_y;
+}
+
+}  // namespace llg
+
+namespace {
+
 // Rust's `{:.3e}`: mantissa with three decimals, exponent without sign padding.
 std::string rust_exp3(double v) {
     char buf[64];
@@ -276,18 +310,10 @@ int llg_demag_op_destroy(llg_demag_op* op) {
 int llg_demag_op_field(llg_demag_op* op, double ms, const double* m_aos, double* b_aos) {
     if (!op || !m_aos || !b_aos) return fail(LLG_ERR_INVALID, "null argument");
     PBC_TRY(cudaSetDevice(op->device));
-    const long long n = (long long)op->nx * op->ny, np = (long long)op->px * op->py;
+    const long long n = (long long)op->nx * op->ny;
     PBC_TRY(cudaMemcpy(op->stage, m_aos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice));
-    k_pbc_pack<<<1184, 256>>>(op->stage, op->nx, op->ny, op->px, op->py, ms, op->M);
-    PBC_TRY(cudaGetLastError());
-    PBC_TRY(llg::launch_fft_strided<double>(op->M, op->px, op->twx, 1, op->py, op->px, 3, np, false, 0));
-    PBC_TRY(llg::launch_fft_strided<double>(op->M, op->py, op->twy, op->px, op->px, 1, 3, np, false, 0));
-    k_pbc_multiply<<<1184, 256>>>(op->K, np, op->M);
-    PBC_TRY(cudaGetLastError());
-    PBC_TRY(llg::launch_fft_strided<double>(op->M, op->px, op->twx, 1, op->py, op->px, 3, np, true, 0));
-    PBC_TRY(llg::launch_fft_strided<double>(op->M, op->py, op->twy, op->px, op->px, 1, 3, np, true, 0));
-    k_pbc_extract<<<1184, 256>>>(op->M, op->nx, op->ny, op->px, op->py, 1.0 / (double)np, op->stage);
-    PBC_TRY(cudaGetLastError());
+    int rc = llg::demag_op_apply_device(op, ms, op->stage, op->stage, 0);
+    if (rc) return rc;
     PBC_TRY(cudaMemcpy(b_aos, op->stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost));
     return LLG_OK;
 }

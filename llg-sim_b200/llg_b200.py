@@ -125,6 +125,12 @@ class MinimizeReport(C.Structure):
                 ("final_max_dm", C.c_double), ("final_tmean", C.c_double), ("final_lambda", C.c_double)]
 
 
+class _AmrPatch(C.Structure):
+    _fields_ = [("i0", C.c_int64), ("j0", C.c_int64), ("cnx", C.c_int64), ("cny", C.c_int64),
+                ("ratio", C.c_int64), ("ghost", C.c_int64), ("m", C.c_void_p), ("geom_mask_fine", C.c_void_p),
+                ("parent_material", C.c_void_p)]
+
+
 class EnergyBreakdown(C.Structure):
     _fields_ = [("exchange", C.c_double), ("anisotropy", C.c_double), ("zeeman", C.c_double),
                 ("dmi", C.c_double), ("demag", C.c_double)]
@@ -199,6 +205,14 @@ def lib():
             "llg_demag_op_kspace": (C.c_int, [vp, dp]),
             "llg_demag_op_save": (C.c_int, [vp, C.c_char_p]),
             "llg_demag_cache_filename": (C.c_int, [P(_Grid), i64, i64, C.c_char_p, i64]),
+            "llg_amr_validated_ratio": (i64, [i64, i64, i64]),
+            "llg_amr_patch_cells": (i64, [P(_AmrPatch)]),
+            "llg_amr_demag_create": (C.c_int, [vp, P(_Grid), i64, P(vp)]),
+            "llg_amr_demag_ratio": (C.c_int, [vp, P(i64)]),
+            "llg_amr_demag_destroy": (C.c_int, [vp]),
+            "llg_amr_restrict_m": (C.c_int, [vp, dp, i32, P(_AmrPatch), dp]),
+            "llg_coarse_fft_demag": (C.c_int, [vp, P(_Material), dp, i32, P(_AmrPatch), dp, dp]),
+            "llg_amr_allfft_demag": (C.c_int, [vp, P(_Material), dp, vp, P(_Grid), dp, dp]),
             "llg_warmstart_param_count": (i64, []),
             "llg_warmstart_create": (C.c_int, [vp, P(C.c_float), i64, P(vp)]),
             "llg_warmstart_destroy": (C.c_int, [vp]),
@@ -589,6 +603,128 @@ class DemagOp:
 
     def save(self, path):
         _check(lib().llg_demag_op_save(self.h, str(path).encode()))
+
+
+class AmrPatch:
+    """Patch2D (amr/patch.rs:15-80) as the demag consumers read it: coarse_rect
+    (i0, j0, cnx, cny) in base cells, ratio relative to the base grid, ghost width,
+    m on the patch grid incl. ghosts ([pny*pnx, 3]), optional fine geometry mask
+    and parent_material flags ([cny*cnx])."""
+
+    def __init__(self, i0, j0, cnx, cny, ratio, ghost, m, geom_mask_fine=None, parent_material=None):
+        self.i0, self.j0, self.cnx, self.cny = int(i0), int(j0), int(cnx), int(cny)
+        self.ratio, self.ghost = int(ratio), int(ghost)
+        self.pnx = self.cnx * self.ratio + 2 * self.ghost
+        self.pny = self.cny * self.ratio + 2 * self.ghost
+        self.m = np.ascontiguousarray(m, dtype=np.float64).reshape(self.pnx * self.pny, 3)
+        self.geom_mask_fine = None if geom_mask_fine is None else \
+            np.ascontiguousarray(np.asarray(geom_mask_fine, dtype=np.uint8).reshape(-1))
+        self.parent_material = None if parent_material is None else \
+            np.ascontiguousarray(np.asarray(parent_material, dtype=np.uint8).reshape(-1))
+
+    def cell_center_xy(self, i, j, base_grid):
+        """Patch2D::cell_center_xy (amr/patch.rs:377-387)."""
+        dx, dy = base_grid.dx / self.ratio, base_grid.dy / self.ratio
+        return ((self.i0 * self.ratio + (i - self.ghost) + 0.5) * dx,
+                (self.j0 * self.ratio + (j - self.ghost) + 0.5) * dy)
+
+    def _c(self):
+        ptr = lambda a: None if a is None else a.ctypes.data
+        return _AmrPatch(self.i0, self.j0, self.cnx, self.cny, self.ratio, self.ghost, self.m.ctypes.data,
+                         ptr(self.geom_mask_fine), ptr(self.parent_material))
+
+
+def _patch_array(patches):
+    arr = (_AmrPatch * max(len(patches), 1))()
+    for q, p in enumerate(patches):
+        arr[q] = p._c()
+    return arr
+
+
+def validated_ratio(nx, ny, ratio):
+    """validated_ratio (coarse_fft_demag.rs:118-150)."""
+    return int(lib().llg_amr_validated_ratio(int(nx), int(ny), int(ratio)))
+
+
+def coarsen_ratio_from_env():
+    """demag_coarsen_ratio (coarse_fft_demag.rs:82-111): LLG_DEMAG_COARSEN_RATIO, 1 when
+    unset, not a positive integer or not a power of two."""
+    raw = os.environ.get("LLG_DEMAG_COARSEN_RATIO")
+    if raw is None:
+        return 1
+    try:
+        r = int(raw.strip())
+    except ValueError:
+        return 1
+    if r < 1 or (r & (r - 1)) != 0:
+        return 1
+    return r
+
+
+class AmrDemag:
+    """Coarse-FFT AMR demag (compute_coarse_fft_demag, coarse_fft_demag.rs:367-511) for
+    one base grid and coarsening ratio, on the GPU."""
+
+    def __init__(self, base_grid, coarsen_ratio=1, device=0):
+        self.base = base_grid
+        h = C.c_void_p()
+        g = base_grid._c()
+        _check(lib().llg_amr_demag_create(_ctx(device), C.byref(g), int(coarsen_ratio), C.byref(h)))
+        self.h = h
+        r = C.c_int64()
+        _check(lib().llg_amr_demag_ratio(self.h, C.byref(r)))
+        self.ratio = r.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().llg_amr_demag_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def restrict_m(self, m_coarse, patches):
+        """restrict_m_to_coarse (coarse_fft_demag.rs:170-240): the enhanced L0 m."""
+        mc = np.ascontiguousarray(m_coarse, dtype=np.float64)
+        out = np.empty((self.base.nx * self.base.ny, 3))
+        _check(lib().llg_amr_restrict_m(self.h, _dp(mc), len(patches), _patch_array(patches), _dp(out)))
+        return out
+
+    def compute(self, material, m_coarse, patches):
+        """Returns (b_coarse [n, 3], [b_patch [pny*pnx, 3] per patch]); without
+        Material::demag the patch list is empty, as in the reference."""
+        mc = np.ascontiguousarray(m_coarse, dtype=np.float64)
+        bc = np.empty((self.base.nx * self.base.ny, 3))
+        cells = [p.pnx * p.pny for p in patches]
+        bp = np.empty((max(sum(cells), 1), 3))
+        mat = material._c()
+        _check(lib().llg_coarse_fft_demag(self.h, C.byref(mat), _dp(mc), len(patches), _patch_array(patches),
+                                          _dp(bc), _dp(bp)))
+        if not material.demag:
+            return bc, []
+        out, o = [], 0
+        for c in cells:
+            out.append(bp[o:o + c].copy())
+            o += c
+        return bc, out
+
+
+def allfft_demag(fine_op, material, m_fine, fine_mask, base_grid):
+    """AllFft branch of AmrStepper::compute_demag (amr/stepper.rs:799-835): returns
+    (b_fine [nf, 3], b_coarse [nb, 3]); fine_op is a DemagOp of the fine grid (pbc 0, 0)."""
+    m = np.ascontiguousarray(m_fine, dtype=np.float64)
+    nf = fine_op.grid.nx * fine_op.grid.ny
+    bf = np.empty((nf, 3))
+    bc = np.empty((base_grid.nx * base_grid.ny, 3))
+    mk = None if fine_mask is None else np.ascontiguousarray(np.asarray(fine_mask, dtype=np.uint8).reshape(-1))
+    mat = material._c()
+    g = base_grid._c()
+    _check(lib().llg_amr_allfft_demag(fine_op.h, C.byref(mat), _dp(m), None if mk is None else mk.ctypes.data,
+                                      C.byref(g), _dp(bf), _dp(bc)))
+    return bf, bc
 
 
 def demag_cache_filename(grid, pbc_x=0, pbc_y=0):

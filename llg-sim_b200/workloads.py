@@ -162,6 +162,60 @@ def holey_film_batch(n, size=128, seed=5):
 
 # ---------------------------------------------------------------------------------------------
 
+class AmrPatchSpec:
+    """One patch of an AMR hierarchy (Patch2D, amr/patch.rs:15-80, as the demag
+    consumers read it)."""
+
+    def __init__(self, i0, j0, cnx, cny, ratio, ghost, m, geom_mask_fine=None, parent_material=None):
+        self.i0, self.j0, self.cnx, self.cny, self.ratio, self.ghost = i0, j0, cnx, cny, ratio, ghost
+        self.pnx, self.pny = cnx * ratio + 2 * ghost, cny * ratio + 2 * ghost
+        self.m, self.geom_mask_fine, self.parent_material = m, geom_mask_fine, parent_material
+
+
+def vortex_field(xs, ys, lx, ly):
+    """m = normalize([-y/r, x/r, 0.3]) at centred, domain-scaled coordinates
+    (the vortex of coarse_fft_demag.rs's tests), vectorised over points."""
+    xr, yr = xs / lx - 0.5, ys / ly - 0.5
+    r = np.maximum(np.hypot(xr, yr), 1e-12)
+    v = np.stack([-yr / r, xr / r, np.full_like(xr, 0.3)], axis=-1)
+    return v / np.linalg.norm(v, axis=-1, keepdims=True)
+
+
+def amr_vortex_hierarchy(nx=192, ny=192, dx=4e-9, dy=4e-9, dz=3e-9, seed=13):
+    """The coarse-FFT demag workload: a vortex in a nx x ny film of dx x dy x dz cells
+    (Ms 8e5), refined around the core by level-1 patches (ratio 2, four 38x38 blocks,
+    15.7 % of the film), level-2 patches (ratio 4, two 19x19 blocks) and one level-3
+    patch (ratio 8, 12x12), ghost 2, fine m = the vortex plus 2 % seeded noise.  The
+    AllFft equivalent is the film at 8x resolution (nx*8 x ny*8, dx/8 x dy/8 x dz),
+    the 1536 x 1536 fine grid of coarse_fft_demag.rs:28-31 for the defaults.
+    Returns (m_coarse [nx*ny, 3], patches in processing order)."""
+    rng = np.random.default_rng(seed)
+    lx, ly = nx * dx, ny * dy
+    i = np.arange(nx)
+    j = np.arange(ny)
+    X, Y = np.meshgrid((i + 0.5) * dx, (j + 0.5) * dy)
+    mc = vortex_field(X, Y, lx, ly).reshape(-1, 3)
+    cx, cy = nx // 2, ny // 2
+    rects = [(cx - 38, cy - 38, 38, 38, 2), (cx, cy - 38, 38, 38, 2), (cx - 38, cy, 38, 38, 2), (cx, cy, 38, 38, 2),
+             (cx - 19, cy - 19, 19, 19, 4), (cx, cy, 19, 19, 4), (cx - 6, cy - 6, 12, 12, 8)]
+    patches = []
+    for (i0, j0, cnx, cny, r) in rects:
+        g = 2
+        pnx, pny = cnx * r + 2 * g, cny * r + 2 * g
+        fi = np.arange(pnx)
+        fj = np.arange(pny)
+        FX, FY = np.meshgrid((i0 * r + (fi - g) + 0.5) * (dx / r), (j0 * r + (fj - g) + 0.5) * (dy / r))
+        v = vortex_field(FX, FY, lx, ly).reshape(-1, 3) + 0.02 * rng.standard_normal((pnx * pny, 3))
+        patches.append(AmrPatchSpec(i0, j0, cnx, cny, r, g, v / np.linalg.norm(v, axis=1, keepdims=True)))
+    return mc, patches
+
+
+def amr_fine_vortex(nx, ny, dx, dy):
+    """The vortex on a uniform fine grid (the flattened hierarchy of the AllFft demag)."""
+    X, Y = np.meshgrid((np.arange(nx) + 0.5) * dx, (np.arange(ny) + 0.5) * dy)
+    return vortex_field(X, Y, nx * dx, ny * dy).reshape(-1, 3)
+
+
 def film_cost(f):
     """Work estimate of one film per step: cells plus its padded transforms,
     2nx x 2ny x log2(2nx x 2ny) (the demag FFTs dominate)."""

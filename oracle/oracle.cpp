@@ -11,10 +11,12 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -1345,10 +1347,17 @@ void orc_restrict_l0_to_demag_grid(int64_t nx_l0, const double* l0_m, int64_t dn
 }
 
 static void uniform_demag(const orc_grid* g, const orc_material* mat, const double* m, double* b) {
-    // compute_demag_field (demag_fft_uniform.rs:146-186): zero, then add unless !mat.demag
-    orc_solver* s = orc_solver_create(g, mat, nullptr);
+    // compute_demag_field (demag_fft_uniform.rs:146-186): zero, then add unless !mat.demag.
+    // Operators are kept per grid as get_demag_operator's cache does (:86-108).
+    static std::map<std::array<double, 5>, std::unique_ptr<orc_solver, void (*)(orc_solver*)>> cache;
+    const std::array<double, 5> key = {(double)g->nx, (double)g->ny, g->dx, g->dy, g->dz};
+    auto it = cache.find(key);
+    if (it == cache.end())
+        it = cache.emplace(key, std::unique_ptr<orc_solver, void (*)(orc_solver*)>(orc_solver_create(g, mat, nullptr),
+                                                                                  orc_solver_destroy)).first;
+    orc_solver* s = it->second.get();
+    s->mat = *mat;
     orc_demag_field(s, m, b);
-    orc_solver_destroy(s);
 }
 
 void orc_coarse_fft_demag(const orc_grid* base, const orc_material* mat, const double* m_coarse,

@@ -63,6 +63,12 @@ class MinimizeReport(C.Structure):
                 ("final_max_dm", C.c_double), ("final_tmean", C.c_double), ("final_lambda", C.c_double)]
 
 
+class AmrPatch(C.Structure):
+    _fields_ = [("i0", C.c_int64), ("j0", C.c_int64), ("cnx", C.c_int64), ("cny", C.c_int64),
+                ("ratio", C.c_int64), ("ghost", C.c_int64), ("m", C.c_void_p), ("geom_mask_fine", C.c_void_p),
+                ("parent_material", C.c_void_p)]
+
+
 class Energy(C.Structure):
     _fields_ = [("exchange", C.c_double), ("anisotropy", C.c_double), ("zeeman", C.c_double),
                 ("dmi", C.c_double), ("demag", C.c_double)]
@@ -99,6 +105,14 @@ def lib():
         L.orc_minimize.argtypes = [vp, dp, C.POINTER(Params), C.c_int, C.POINTER(MinimizeSettings),
                                    C.POINTER(MinimizeReport)]
         L.orc_default_minimize_settings.argtypes = [C.POINTER(MinimizeSettings)]
+        L.orc_validated_ratio.restype = C.c_int64
+        L.orc_validated_ratio.argtypes = [C.c_int64, C.c_int64, C.c_int64]
+        L.orc_sample_bilinear.argtypes = [C.POINTER(Grid), dp, C.c_double, C.c_double, dp]
+        L.orc_restrict_m_to_coarse.argtypes = [C.POINTER(Grid), dp, C.c_int32, C.POINTER(AmrPatch), dp]
+        L.orc_restrict_l0_to_demag_grid.argtypes = [C.c_int64, dp, C.c_int64, C.c_int64, C.c_int64, dp]
+        L.orc_coarse_fft_demag.argtypes = [C.POINTER(Grid), C.POINTER(Material), dp, C.c_int32,
+                                           C.POINTER(AmrPatch), C.c_int64, dp, dp]
+        L.orc_allfft_demag.argtypes = [C.POINTER(Grid), C.POINTER(Material), dp, vp, C.POINTER(Grid), dp, dp]
         L.orc_energy_breakdown.argtypes = [vp, dp, dp, C.POINTER(Energy)]
         L.orc_torque_metric.restype = C.c_double
         L.orc_torque_metric.argtypes = [C.c_int64, dp, dp, C.c_int]
@@ -179,6 +193,78 @@ def default_minimize_settings(**kw):
         else:
             setattr(s, k, v)
     return s
+
+
+# ---------------------------------------------------------------- AMR demag consumers
+
+def _patches(patches):
+    """patches: objects with i0, j0, cnx, cny, ratio, ghost, m ([pny*pnx, 3] float64),
+    geom_mask_fine / parent_material (uint8 arrays or None)."""
+    arr = (AmrPatch * max(len(patches), 1))()
+    keep = []
+    for q, p in enumerate(patches):
+        m = np.ascontiguousarray(p.m, dtype=np.float64)
+        gm = None if p.geom_mask_fine is None else np.ascontiguousarray(p.geom_mask_fine, dtype=np.uint8)
+        pm = None if p.parent_material is None else np.ascontiguousarray(p.parent_material, dtype=np.uint8)
+        keep += [m, gm, pm]
+        arr[q] = AmrPatch(p.i0, p.j0, p.cnx, p.cny, p.ratio, p.ghost, m.ctypes.data,
+                          None if gm is None else gm.ctypes.data, None if pm is None else pm.ctypes.data)
+    return arr, keep
+
+
+def validated_ratio(nx, ny, ratio):
+    return int(lib().orc_validated_ratio(int(nx), int(ny), int(ratio)))
+
+
+def sample_bilinear(grid, field, x, y):
+    f = np.ascontiguousarray(field, dtype=np.float64)
+    out = np.empty(3)
+    lib().orc_sample_bilinear(C.byref(grid), _dp(f), float(x), float(y), _dp(out))
+    return out
+
+
+def restrict_m_to_coarse(base, m_coarse, patches):
+    mc = np.ascontiguousarray(m_coarse, dtype=np.float64)
+    out = np.empty((base.nx * base.ny, 3))
+    arr, keep = _patches(patches)
+    lib().orc_restrict_m_to_coarse(C.byref(base), _dp(mc), len(patches), arr, _dp(out))
+    return out
+
+
+def restrict_l0_to_demag_grid(nx_l0, l0_m, dnx, dny, ratio):
+    m = np.ascontiguousarray(l0_m, dtype=np.float64)
+    out = np.empty((dnx * dny, 3))
+    lib().orc_restrict_l0_to_demag_grid(int(nx_l0), _dp(m), int(dnx), int(dny), int(ratio), _dp(out))
+    return out
+
+
+def coarse_fft_demag(base, material, m_coarse, patches, ratio=1):
+    """compute_coarse_fft_demag (coarse_fft_demag.rs:367-511) with an explicit ratio:
+    (b_coarse, [b_patch per patch]) — no patch fields without Material::demag."""
+    mc = np.ascontiguousarray(m_coarse, dtype=np.float64)
+    bc = np.empty((base.nx * base.ny, 3))
+    cells = [(p.cny * p.ratio + 2 * p.ghost) * (p.cnx * p.ratio + 2 * p.ghost) for p in patches]
+    bp = np.zeros((max(sum(cells), 1), 3))
+    arr, keep = _patches(patches)
+    lib().orc_coarse_fft_demag(C.byref(base), C.byref(material), _dp(mc), len(patches), arr, int(ratio), _dp(bc),
+                               _dp(bp))
+    if not material.demag:
+        return bc, []
+    out, o = [], 0
+    for c in cells:
+        out.append(bp[o:o + c].copy())
+        o += c
+    return bc, out
+
+
+def allfft_demag(fine, material, m_fine, fine_mask, base):
+    m = np.ascontiguousarray(m_fine, dtype=np.float64)
+    bf = np.empty((fine.nx * fine.ny, 3))
+    bc = np.empty((base.nx * base.ny, 3))
+    mk = None if fine_mask is None else np.ascontiguousarray(np.asarray(fine_mask, dtype=np.uint8).reshape(-1))
+    lib().orc_allfft_demag(C.byref(fine), C.byref(material), _dp(m), None if mk is None else mk.ctypes.data,
+                           C.byref(base), _dp(bf), _dp(bc))
+    return bf, bc
 
 
 class Solver:
