@@ -401,6 +401,28 @@ def amr_leg(L, reps=5):
     return out
 
 
+def sp4_leg(L):
+    """The µMAG SP4 driver flow (st_problems/sp4.rs) end to end through the public API:
+    relax, then 1 ns of RK45 under field a with 10 ps samples, table.csv and the text
+    OVF snapshots written to a temporary directory; wall clock per precision."""
+    import tempfile
+    import time
+
+    import sp4
+
+    out = {"workload": "SP4a: 200x50x1 cells of 2.5x2.5x3 nm, relax to max|m x B| 1e-4 T, 1 ns RK45 at "
+                       "(-24.6, 4.3, 0) mT, table every 10 ps, OVF every 100 ps"}
+    for name, prec in (("fp32", L.FP32), ("fp64", L.FP64)):
+        with tempfile.TemporaryDirectory() as d:
+            t0 = time.perf_counter()
+            r = sp4.run_sp4("a", d, precision=prec, log=lambda *a: None)
+            wall = time.perf_counter() - t0
+        out[name] = {"wall_s": wall, "relax_steps": int(r["relax_accepted"]), "run_steps": r["run_accepted"],
+                     "run_rejected": r["run_rejected"], "crossover_t_s": r["crossover_t"],
+                     "mean_m_final": [float(x) for x in r["rows"][-1][1:]], "ovf_snapshots": r["snapshots"]}
+    return out
+
+
 def reduce_over_ranks(dist, x, op, device):
     """x reduced over the process group (op "max" or "sum"); x itself without one."""
     if dist is None:
@@ -579,6 +601,9 @@ def run_gpu(args):
     amr = None
     if not args.no_amr and world == 1:
         amr = amr_leg(L)
+    sp4r = None
+    if not args.no_sp4 and world == 1:
+        sp4r = sp4_leg(L)
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -594,7 +619,7 @@ def run_gpu(args):
                            "l2": "inputs larger than L2: ~190 MB per film working set (m, 7 torques, stage states, "
                                  "25 MB spectrum, 16 MB kernel) vs 126 MB L2"},
                 "clocks": clk, "gpu_launches": launches, "roofline": roofline, "roofline_step": roofline_step,
-                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "warm_start": warm, "amr_demag": amr,
+                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "warm_start": warm, "amr_demag": amr, "sp4": sp4r,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     s.close()
@@ -619,6 +644,7 @@ def main():
     ap.add_argument("--no-flow", action="store_true")
     ap.add_argument("--no-warmstart", action="store_true")
     ap.add_argument("--no-amr", action="store_true")
+    ap.add_argument("--no-sp4", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -359,6 +359,29 @@ int llg_coarse_fft_demag(llg_amr_demag* h, const llg_material* mat, const double
 int llg_amr_allfft_demag(llg_demag_op* fine_op, const llg_material* mat, const double* m_fine,
                          const uint8_t* fine_mask, const llg_grid* base, double* b_fine, double* b_coarse);
 
+/* ---------------- OVF 2.0 writers (ovf.rs:17-251) ----------------
+ * OvfMeta (ovf.rs:17-45): title, "# Desc:" lines, value labels and units.
+ * Formats: LLG_OVF_TEXT = write_ovf2_rectangular_text (:54-151),
+ * LLG_OVF_BINARY4 = write_ovf2_rectangular_binary4 (:153-251); byte-identical to
+ * the reference's files.  The parent directory is created as needed. */
+enum { LLG_OVF_TEXT = 0, LLG_OVF_BINARY4 = 1 };
+typedef struct llg_ovf_meta {
+    const char* title;
+    const char* const* desc_lines;
+    int32_t n_desc;
+    const char* valuelabels[3];
+    const char* valueunits[3];
+} llg_ovf_meta;
+/* a host field (AoS FP64 [nx*ny][3]) */
+int llg_ovf2_write(const char* path, const llg_grid* g, const double* m_aos, const llg_ovf_meta* meta,
+                   int32_t format);
+/* the solver's resident m; binary4 is packed to f32 on the GPU (12 bytes per cell cross the bus) */
+int llg_ovf2_write_state(llg_solver* s, const char* path, const llg_ovf_meta* meta, int32_t format);
+int llg_batch_ovf2_write_state(llg_batch* b, int32_t film, const char* path, const llg_ovf_meta* meta,
+                               int32_t format);
+/* Rust's `{:.<precision>e}` of v (the number format of the OVF headers and text data) */
+int llg_ovf_format_exp(double v, int32_t precision, char* buf, int64_t len);
+
 typedef struct llg_warmstart llg_warmstart;
 int64_t llg_warmstart_param_count(void);
 int llg_warmstart_create(llg_ctx* ctx, const float* params, int64_t n_params, llg_warmstart** out);

@@ -31,6 +31,9 @@ cudaError_t build_demag_kernel(int nx, int ny, double dx, double dy, double dz, 
 int demag_op_apply_device(llg_demag_op* op, double ms, const double* d_m_aos, double* d_b_aos, cudaStream_t s);
 void demag_op_info(const llg_demag_op* op, int* device, llg_grid* g, int* pbc_x, int* pbc_y);
 
+// OVF 2.0 binary4 file of a packed payload (3*nx*ny f32, x, y, z per cell).
+int ovf2_write_packed(const char* path, const llg_grid* g, const float* payload, const llg_ovf_meta* meta);
+
 // Launch geometry of one film set.
 struct LaunchGeom {
     const FilmDev* films;

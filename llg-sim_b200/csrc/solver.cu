@@ -207,6 +207,19 @@ __global__ void k_aos_to_soa(const FilmDev* films, int film, const double* __res
     }
 }
 
+// The resident m as AoS f32 (the OVF binary4 payload), rounded to nearest.
+template <typename R>
+__global__ void k_soa_to_aos_f32(const FilmDev* films, int film, float* __restrict__ dst) {
+    const FilmDev& F = films[film];
+    const int n = F.nx * F.ny;
+    const R* src = mbuf<R>(F, MB_M0, F.st->cur);
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        dst[idx * 3 + 0] = (float)src[idx];
+        dst[idx * 3 + 1] = (float)src[n + idx];
+        dst[idx * 3 + 2] = (float)src[2 * n + idx];
+    }
+}
+
 template <typename R>
 __global__ void k_soa_to_aos(const FilmDev* films, int film, int which, double* __restrict__ dst) {
     const FilmDev& F = films[film];
@@ -230,6 +243,7 @@ struct EngineBase {
     virtual int sync() = 0;
     virtual int set_state(int f, const double* m) = 0;
     virtual int get_state(int f, double* m) = 0;
+    virtual int write_ovf(int f, const char* path, const llg_ovf_meta* meta, int format) = 0;
     virtual int mean_m(double* out3n) = 0;
     virtual int build_h_eff(int f, const llg_params* p, int fmask, double* b) = 0;
     virtual int demag_field(int f, double* b) = 0;
@@ -742,6 +756,24 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaStreamSynchronize(stream));
         if (ws::net_error()) return set_error(LLG_ERR_TIMEOUT, "warm-start network: tensor-core wait timed out");
         return LLG_OK;
+    }
+
+    int write_ovf(int f, const char* path, const llg_ovf_meta* meta, int format) override {
+        if (format == LLG_OVF_TEXT) {
+            std::vector<double> m(3 * (size_t)cells(f));
+            int rc = get_state(f, m.data());
+            return rc ? rc : llg_ovf2_write(path, &grids[f], m.data(), meta, format);
+        }
+        if (format != LLG_OVF_BINARY4) return set_error(LLG_ERR_INVALID, "unknown OVF format %d", format);
+        int rc;
+        if ((rc = ensure_stage())) return rc;
+        k_soa_to_aos_f32<R><<<592, 256, 0, stream>>>(d_films, f, reinterpret_cast<float*>(d_stage));
+        CUDA_TRY(cudaGetLastError());
+        std::vector<float> payload(3 * (size_t)cells(f));
+        CUDA_TRY(cudaMemcpyAsync(payload.data(), d_stage, sizeof(float) * payload.size(), cudaMemcpyDeviceToHost,
+                                 stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return ovf2_write_packed(path, &grids[f], payload.data(), meta);
     }
 
     int get_state(int f, double* m) override {
@@ -1547,6 +1579,11 @@ int llg_get_state(llg_solver* s, double* m) {
     if (!rc && !m) rc = set_error(LLG_ERR_INVALID, "null m");
     return rc ? rc : s->eng->get_state(0, m);
 }
+int llg_ovf2_write_state(llg_solver* s, const char* path, const llg_ovf_meta* meta, int32_t format) {
+    int rc = bind(s);
+    if (!rc && (!path || !meta)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc : s->eng->write_ovf(0, path, meta, format);
+}
 int llg_mean_m(llg_solver* s, double out3[3]) {
     int rc = bind(s);
     return rc ? rc : s->eng->mean_m(out3);
@@ -1730,6 +1767,13 @@ int llg_batch_minimize(llg_batch* b, const llg_params* params, int32_t fmask, co
     int rc = bind(b);
     if (!rc && (!params || !settings || !reports)) rc = set_error(LLG_ERR_INVALID, "null argument");
     return rc ? rc : b->eng->minimize(params, fmask, settings, reports);
+}
+int llg_batch_ovf2_write_state(llg_batch* b, int32_t film, const char* path, const llg_ovf_meta* meta,
+                               int32_t format) {
+    int rc = bind(b);
+    if (!rc && (!path || !meta)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    if (!rc && (film < 0 || film >= b->eng->nfilms())) rc = set_error(LLG_ERR_INVALID, "bad film %d", film);
+    return rc ? rc : b->eng->write_ovf(film, path, meta, format);
 }
 int llg_batch_compute_energy(llg_batch* b, const double* b_ext, llg_energy_breakdown* out) {
     int rc = bind(b);

@@ -24,6 +24,7 @@ EXCH_ANIS, EXCH_ANIS_DMI, FULL = 0, 1, 2
 # TorqueMetric (relax.rs:32-37)
 TORQUE_MAX, TORQUE_MEAN, TORQUE_RMS, TORQUE_MEANSQ = 0, 1, 2, 3
 FP32, FP64 = 0, 1
+OVF_TEXT, OVF_BINARY4 = 0, 1              # write_ovf2_rectangular_text / _binary4 (ovf.rs:54,153)
 MU0 = 4.0 * np.pi * 1e-7                  # params.rs:15
 GAMMA_E_RAD_PER_S_T = 1.76085963023e11     # params.rs:16
 
@@ -131,6 +132,11 @@ class _AmrPatch(C.Structure):
                 ("parent_material", C.c_void_p)]
 
 
+class _OvfMeta(C.Structure):
+    _fields_ = [("title", C.c_char_p), ("desc_lines", C.POINTER(C.c_char_p)), ("n_desc", C.c_int32),
+                ("valuelabels", C.c_char_p * 3), ("valueunits", C.c_char_p * 3)]
+
+
 class EnergyBreakdown(C.Structure):
     _fields_ = [("exchange", C.c_double), ("anisotropy", C.c_double), ("zeeman", C.c_double),
                 ("dmi", C.c_double), ("demag", C.c_double)]
@@ -205,6 +211,10 @@ def lib():
             "llg_demag_op_kspace": (C.c_int, [vp, dp]),
             "llg_demag_op_save": (C.c_int, [vp, C.c_char_p]),
             "llg_demag_cache_filename": (C.c_int, [P(_Grid), i64, i64, C.c_char_p, i64]),
+            "llg_ovf2_write": (C.c_int, [C.c_char_p, P(_Grid), dp, P(_OvfMeta), i32]),
+            "llg_ovf2_write_state": (C.c_int, [vp, C.c_char_p, P(_OvfMeta), i32]),
+            "llg_batch_ovf2_write_state": (C.c_int, [vp, i32, C.c_char_p, P(_OvfMeta), i32]),
+            "llg_ovf_format_exp": (C.c_int, [C.c_double, i32, C.c_char_p, i64]),
             "llg_amr_validated_ratio": (i64, [i64, i64, i64]),
             "llg_amr_patch_cells": (i64, [P(_AmrPatch)]),
             "llg_amr_demag_create": (C.c_int, [vp, P(_Grid), i64, P(vp)]),
@@ -410,6 +420,11 @@ class Solver:
         _check(lib().llg_minimize(self.h, C.byref(p), int(field_mask), C.byref(settings), C.byref(rep)))
         return rep
 
+    def write_ovf2(self, path, meta, fmt=OVF_BINARY4):
+        """OVF 2.0 file of the resident m (write_ovf2_rectangular_binary4 / _text, ovf.rs:54-251)."""
+        cm = meta._c()
+        _check(lib().llg_ovf2_write_state(self.h, str(path).encode(), C.byref(cm), int(fmt)))
+
     def compute_energy(self, b_ext):
         be = np.ascontiguousarray(np.asarray(b_ext, dtype=np.float64).reshape(3))
         e = EnergyBreakdown()
@@ -535,6 +550,10 @@ class Batch:
         reps = (MinimizeReport * self.n)()
         _check(lib().llg_batch_minimize(self.h, P, int(field_mask), C.byref(settings), reps))
         return list(reps)
+
+    def write_ovf2(self, f, path, meta, fmt=OVF_BINARY4):
+        cm = meta._c()
+        _check(lib().llg_batch_ovf2_write_state(self.h, int(f), str(path).encode(), C.byref(cm), int(fmt)))
 
     def warm_start(self, net, b_exts):
         """Replace every film's state by the warm-start network's proposal (on the device)."""
@@ -725,6 +744,86 @@ def allfft_demag(fine_op, material, m_fine, fine_mask, base_grid):
     _check(lib().llg_amr_allfft_demag(fine_op.h, C.byref(mat), _dp(m), None if mk is None else mk.ctypes.data,
                                       C.byref(g), _dp(bf), _dp(bc)))
     return bf, bc
+
+
+# ------------------------------------------------------------------ OVF 2.0 (ovf.rs)
+
+
+def rust_exp(v, precision):
+    """Rust's `{:.<precision>e}` of v (llg_ovf_format_exp)."""
+    buf = C.create_string_buffer(96)
+    _check(lib().llg_ovf_format_exp(float(v), int(precision), buf, 96))
+    return buf.value.decode()
+
+
+class OvfMeta:
+    """OvfMeta (ovf.rs:17-45)."""
+
+    def __init__(self, title="", desc_lines=None, valuelabels=("", "", ""), valueunits=("", "", "")):
+        self.title = title
+        self.desc_lines = list(desc_lines or [])
+        self.valuelabels = tuple(valuelabels)
+        self.valueunits = tuple(valueunits)
+
+    @classmethod
+    def magnetization(cls):
+        return cls("m", [], ("m_x", "m_y", "m_z"), ("1", "1", "1"))
+
+    def with_total_sim_time(self, t_s):
+        """MuMax-style time line (ovf.rs:36-40)."""
+        self.desc_lines.append(f"Total simulation time:  {rust_exp(t_s, 16)}  s")
+        return self
+
+    def push_desc_line(self, s):
+        self.desc_lines.append(str(s))
+
+    def _c(self):
+        enc = lambda x: str(x).encode()
+        self._keep = (C.c_char_p * max(len(self.desc_lines), 1))(*[enc(d) for d in self.desc_lines])
+        return _OvfMeta(enc(self.title), self._keep, len(self.desc_lines),
+                        (C.c_char_p * 3)(*[enc(x) for x in self.valuelabels]),
+                        (C.c_char_p * 3)(*[enc(x) for x in self.valueunits]))
+
+
+def write_ovf2_rectangular_text(path, grid, m, meta):
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    g, cm = grid._c(), meta._c()
+    _check(lib().llg_ovf2_write(str(path).encode(), C.byref(g), _dp(m), C.byref(cm), OVF_TEXT))
+
+
+def write_ovf2_rectangular_binary4(path, grid, m, meta):
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    g, cm = grid._c(), meta._c()
+    _check(lib().llg_ovf2_write(str(path).encode(), C.byref(g), _dp(m), C.byref(cm), OVF_BINARY4))
+
+
+class OvfSeries:
+    """OvfSeries (ovf.rs:255-316): binary4 dumps every `every` seconds of simulated
+    time.  `write(path, meta)` writes the current state (e.g. a Solver's
+    write_ovf2 with OVF_BINARY4)."""
+
+    def __init__(self, directory, every_s):
+        os.makedirs(directory, exist_ok=True)
+        self.dir = directory
+        self.every = max(float(every_s), 0.0)
+        self.next_dump = 0.0
+        self.frame = 0
+
+    def dump_initial(self, write, make_path, meta):
+        self.next_dump = 0.0
+        write(make_path(self.frame, 0.0), meta)
+        self.frame += 1
+        self.next_dump = self.every
+
+    def maybe_dump_due(self, write, t_approx, make_path, meta_builder):
+        if self.every <= 0.0:
+            return
+        eps = 1e-15
+        while t_approx + eps >= self.next_dump:
+            t = self.next_dump
+            write(make_path(self.frame, t), meta_builder(t))
+            self.frame += 1
+            self.next_dump += self.every
 
 
 def demag_cache_filename(grid, pbc_x=0, pbc_y=0):
