@@ -1116,7 +1116,8 @@ struct Engine final : EngineBase {
         if (fmask < 0 || fmask > 2) return set_error(LLG_ERR_INVALID, "bad field mask %d", fmask);
         int rc;
         if ((rc = apply_params(p))) return rc;
-        RelaxSettingsDev S{};
+        RelaxSettingsDev S;
+        std::memset(&S, 0, sizeof(S));   // padding too: the graph cache compares settings bytewise
         S.max_err = st->max_err;
         S.headroom = st->headroom;
         S.dt_min = st->dt_min;
@@ -1221,7 +1222,8 @@ struct Engine final : EngineBase {
         if (fmask < 0 || fmask > 2) return set_error(LLG_ERR_INVALID, "bad field mask %d", fmask);
         int rc;
         if ((rc = apply_params(p))) return rc;
-        MinimizeSettingsDev S{};
+        MinimizeSettingsDev S;
+        std::memset(&S, 0, sizeof(S));   // padding too: the graph cache compares settings bytewise
         S.thr = st->torque_threshold;
         S.lambda0 = st->lambda0;
         S.lambda_min = st->lambda_min;
