@@ -401,6 +401,59 @@ def amr_leg(L, reps=5):
     return out
 
 
+def minimize_leg(L, torch, stream, iters=300):
+    """minimize_damping_only on the 1024x1024 film of the main workload (FP32 and FP64,
+    random m0), a fixed number of iterations (threshold and dM stop out of reach),
+    device-clock time per iteration; the FP64 oracle times three iterations on the host.
+    An iteration is one field build plus the update: m in, spectrum out and back, kernel
+    planes, m' out = 148 B per cell as one RK stage evaluation."""
+    import time
+
+    w = WORKLOAD
+    n = w["nx"] * w["ny"]
+    g = L.Grid2D(w["nx"], w["ny"], w["dx"], w["dy"], w["dz"])
+    mat = L.Material(w["ms"], w["a_ex"], w["k_u"], w["easy"], w["dmi"], True)
+    p = L.LLGParams(GAMMA, w["alpha"], w["dt0"], w["b_ext"])
+    st = L.MinimizeSettings.default(max_iters=iters, torque_threshold=0.0, dm_stop=None, stall_iters=10 ** 9)
+    pk, _ = peaks()
+    out = {"workload": workload_desc().split(", RK45")[0] + f", {iters} minimiser iterations (lambda0 2e-2)"}
+    for name, prec in (("fp32", L.FP32), ("fp64", L.FP64)):
+        s = L.Solver(g, mat, prec)
+        s.set_stream(stream.cuda_stream)
+        s.set_state(L.init_random(n, w["seed"]))
+        s.minimize(p, L.FULL, L.MinimizeSettings.default(max_iters=3, torque_threshold=0.0, dm_stop=None))
+        s.set_state(L.init_random(n, w["seed"]))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = s.minimize(p, L.FULL, st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        it = max(int(r.iters), 1)
+        out[name] = {"iters": int(r.iters), "ms_per_iter": ms / it, "cell_iters_per_s": n * it / (ms * 1e-3),
+                     "achieved_gbs": 148.0 * n * it / (ms * 1e-3) / 1e9, "final_torque": r.final_torque,
+                     "final_tmean": r.final_tmean, "final_lambda": r.final_lambda}
+        out[name]["hbm_frac"] = out[name]["achieved_gbs"] / pk
+        s.close()
+    try:
+        import oracle as O
+
+        O.set_threads(os.cpu_count() or 1)
+        og = O.make_grid(w["nx"], w["ny"], w["dx"], w["dy"], w["dz"])
+        osv = O.Solver(og, O.make_material(w["ms"], w["a_ex"], w["k_u"], w["easy"], w["dmi"], True))
+        m = O.init_random(n, w["seed"])
+        op = O.make_params(GAMMA, w["alpha"], w["dt0"], w["b_ext"])
+        osv.build_h_eff(m, w["b_ext"], 2)            # kernel built outside the timed region
+        t0 = time.perf_counter()
+        osv.minimize(m, op, 2, O.default_minimize_settings(max_iters=3, torque_threshold=0.0, dm_stop=None))
+        el = time.perf_counter() - t0
+        out["cpu_oracle"] = {"ms_per_iter": el / 3 * 1e3, "cell_iters_per_s": n * 3 / el, "threads": O.get_threads()}
+    except Exception as exc:   # the oracle library is optional on a GPU box
+        out["cpu_oracle"] = f"unavailable: {exc}"
+    return out
+
+
 def sp4_leg(L):
     """The µMAG SP4 driver flow (st_problems/sp4.rs) end to end through the public API:
     relax, then 1 ns of RK45 under field a with 10 ps samples, table.csv and the text
@@ -604,6 +657,9 @@ def run_gpu(args):
     sp4r = None
     if not args.no_sp4 and world == 1:
         sp4r = sp4_leg(L)
+    mini = None
+    if not args.no_minimize and world == 1:
+        mini = minimize_leg(L, torch, stream)
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -619,7 +675,7 @@ def run_gpu(args):
                            "l2": "inputs larger than L2: ~190 MB per film working set (m, 7 torques, stage states, "
                                  "25 MB spectrum, 16 MB kernel) vs 126 MB L2"},
                 "clocks": clk, "gpu_launches": launches, "roofline": roofline, "roofline_step": roofline_step,
-                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "warm_start": warm, "amr_demag": amr, "sp4": sp4r,
+                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "warm_start": warm, "amr_demag": amr, "sp4": sp4r, "minimize": mini,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
     s.close()
@@ -645,6 +701,7 @@ def main():
     ap.add_argument("--no-warmstart", action="store_true")
     ap.add_argument("--no-amr", action="store_true")
     ap.add_argument("--no-sp4", action="store_true")
+    ap.add_argument("--no-minimize", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -155,18 +155,30 @@ __global__ void k_controller(FilmDev* films, int nfilms, int order, int req) {
 }
 
 // Sum the per-block partial reductions of each film in block order (deterministic).
+// One warp per film: lane l sums blocks l, l + 32, ... in order, then a fixed
+// butterfly combines the lanes (deterministic; the loads of the 32 lanes overlap).
+constexpr int kFinalizeFilmsPerBlock = 4;
 __global__ void k_finalize(FilmDev* films, int nfilms, int req) {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= nfilms) return;
+    const int f = blockIdx.x * kFinalizeFilmsPerBlock + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (f >= nfilms) return;   // uniform over the warp
     const FilmDev& F = films[f];
     if (req && (!F.st->active || F.st->req != req)) return;
     double acc[RED_NSLOT];
+#pragma unroll
     for (int s = 0; s < RED_NSLOT; ++s) acc[s] = 0.0;
-    for (int b = 0; b < F.nblk; ++b) {
+    for (int b = lane; b < F.nblk; b += 32) {
         const double* p = F.red_part + (size_t)b * RED_NSLOT;
+#pragma unroll
         for (int s = 0; s < RED_NSLOT; ++s) acc[s] = (s == RED_TMAX) ? fmax(acc[s], p[s]) : acc[s] + p[s];
     }
-    for (int s = 0; s < RED_NSLOT; ++s) F.st->red[s] = acc[s];
+#pragma unroll
+    for (int s = 0; s < RED_NSLOT; ++s)
+        for (int o = 16; o > 0; o >>= 1) {
+            const double w = __shfl_xor_sync(0xffffffffu, acc[s], o);
+            acc[s] = (s == RED_TMAX) ? fmax(acc[s], w) : acc[s] + w;
+        }
+    if (lane == 0)
+        for (int s = 0; s < RED_NSLOT; ++s) F.st->red[s] = acc[s];
 }
 
 // <m> partial sums per row block of every film.
@@ -789,7 +801,8 @@ struct Engine final : EngineBase {
     int mean_m(double* out3n) override {
         k_mean_m<R><<<std::min(geom.n_row_items, 148 * 8), 256, 0, stream>>>(d_films, d_row_items, geom.n_row_items);
         CUDA_TRY(cudaGetLastError());
-        k_finalize<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, 0);
+        k_finalize<<<(nf + kFinalizeFilmsPerBlock - 1) / kFinalizeFilmsPerBlock, 32 * kFinalizeFilmsPerBlock, 0,
+                     stream>>>(d_films, nf, 0);
         CUDA_TRY(cudaGetLastError());
         int rc;
         if ((rc = read_states())) return rc;
@@ -837,7 +850,8 @@ struct Engine final : EngineBase {
     }
 
     int finalize(int req) {
-        k_finalize<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, req);
+        k_finalize<<<(nf + kFinalizeFilmsPerBlock - 1) / kFinalizeFilmsPerBlock, 32 * kFinalizeFilmsPerBlock, 0,
+                     stream>>>(d_films, nf, req);
         CUDA_TRY(cudaGetLastError());
         launches += 1;
         return LLG_OK;
