@@ -330,7 +330,7 @@ def warmstart_leg(L, torch, stream, max_over_ranks, n_films=16, size=256):
                 eo = s.energy(states[i], f.b_ext).total()
                 worst = max(worst, abs(en[i] - eo) / abs(eo))
         out["energy_max_rel_diff_vs_fp64_oracle"] = worst
-    except Exception as exc:   # the oracle library is optional on a GPU box
+    except Exception as exc:   # the oracle library is optional where the benchmark runs
         out["energy_max_rel_diff_vs_fp64_oracle"] = f"unavailable: {exc}"
     return out
 
@@ -396,7 +396,7 @@ def amr_leg(L, reps=5):
         out["cpu_coarse_fft_ms"] = (time.perf_counter() - t0) * 1e3
         out["cpu_threads"] = O.get_threads()
         out["coarse_max_rel_diff_vs_fp64_oracle"] = float(np.abs(bc - oc).max() / np.abs(oc).max())
-    except Exception as exc:   # the oracle library is optional on a GPU box
+    except Exception as exc:   # the oracle library is optional where the benchmark runs
         out["cpu_coarse_fft_ms"] = f"unavailable: {exc}"
     return out
 
@@ -449,7 +449,7 @@ def minimize_leg(L, torch, stream, iters=300):
         osv.minimize(m, op, 2, O.default_minimize_settings(max_iters=3, torque_threshold=0.0, dm_stop=None))
         el = time.perf_counter() - t0
         out["cpu_oracle"] = {"ms_per_iter": el / 3 * 1e3, "cell_iters_per_s": n * 3 / el, "threads": O.get_threads()}
-    except Exception as exc:   # the oracle library is optional on a GPU box
+    except Exception as exc:   # the oracle library is optional where the benchmark runs
         out["cpu_oracle"] = f"unavailable: {exc}"
     return out
 

@@ -180,7 +180,7 @@ int llg_step_rk23_relax(llg_solver* s, llg_params* params, int32_t field_mask, d
 
 /* Device-resident RK45 integration: repeats attempts on the GPU without host
  * round trips until `n_accepted` more steps are accepted or the simulated time
- * reaches t_end, measured from the start of this call (dt is clamped to land on t_end, as the drivers do in
+ * reaches t_end, measured from the start of this call (dt is clamped to land on t_end, as the reference drivers do in
  * st_problems/sp4.rs:308-314).  Pass n_accepted < 0 or t_end = +inf to disable
  * either limit.  max_attempts bounds the work. */
 int llg_run_rk45(llg_solver* s, llg_params* params, int32_t field_mask, double max_err, double headroom,

@@ -1500,7 +1500,7 @@ int check_device(int device) {
     if (device < 0 || device >= count) return set_error(LLG_ERR_INVALID, "device %d out of range (%d)", device, count);
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return set_error(LLG_ERR_CUDA, "cudaGetDeviceProperties");
-    if (prop.major != 10) return set_error(LLG_ERR_NO_DEVICE, "device %d is sm_%d%d; this build targets sm_100a", device,
+    if (prop.major != 10) return set_error(LLG_ERR_NO_DEVICE, "device %d is sm_%d%d; the library is compiled for sm_100a", device,
                                            prop.major, prop.minor);
     return LLG_OK;
 }

@@ -26,7 +26,7 @@ def test_sp4_short_run_outputs(gpu, tmp_path):
     # the last snapshot is the final state: its mean equals the table's last row
     text = (tmp_path / "sp4a" / "m0000002.ovf").read_text().splitlines()
     assert text[0] == "# OOMMF OVF 2.0"
-    # the snapshot time is k * dt_out as the driver computes it (sp4.rs:309)
+    # the snapshot time is k * dt_out as sp4.rs:309 computes it
     assert "# Desc: Total simulation time:  " + R.rust_exp(10 * 1e-11, 16) + "  s" in text
     i0 = text.index("# Begin: Data Text") + 1
     data = np.array([[float(x) for x in ln.split()] for ln in text[i0:i0 + 200 * 50]])
