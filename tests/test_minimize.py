@@ -298,3 +298,57 @@ def test_relax_until_gate_on_oracle(orc):
     assert all(r.has_final_torque_max for r in out.relax_passes)
     assert out.gate_passed == E.gate_ok(out.relax_passes[-1], gate)
     assert np.allclose(np.linalg.norm(osv.m, axis=1), 1.0)
+
+
+# ------------------------------------------------------------------ policies (equilibrate.rs:261-430)
+
+def test_policy_defaults(gpu):
+    """RemanencePolicy / HysteresisPolicy / RelaxGate defaults (equilibrate.rs:60-77, 270-300, 341-382)."""
+    g = E.RelaxGate()
+    assert (g.torque_gate, g.torque_gate_max, g.extra_passes, g.fallback_to_minimize,
+            g.extra_pass_max_steps_mult) == (None, None, 2, False, 2.0)
+    ms = g.minimize_settings()
+    assert (ms.max_iters, ms.torque_threshold, ms.lambda0, ms.dm_stop) == (200, 8e-4, 2e-2, 1e-6)
+    r = E.RemanencePolicy.default()
+    assert r.reset_dt and r.gate.torque_gate == 5e-4 and r.gate.torque_gate_max is None
+    st = r.relax
+    assert (st.phase1_enabled, st.phase2_enabled, st.torque_metric, st.has_torque_threshold) == (1, 1, 1, 0)
+    assert (st.torque_plateau_checks, st.torque_plateau_min_checks, st.torque_plateau_rel,
+            st.torque_plateau_abs, st.max_err) == (8, 8, 0.0, 1e-7, 1e-5)
+    h = E.HysteresisPolicy.default()
+    assert h.premin is None and h.warm_start_dt and h.gate.torque_gate == 8e-4 and h.gate.torque_gate_max is None
+    st = h.relax
+    assert (st.phase1_enabled, st.phase2_enabled, st.torque_metric, st.has_torque_threshold) == (0, 1, 1, 0)
+    assert (st.torque_plateau_checks, st.torque_plateau_min_checks, st.torque_plateau_rel,
+            st.torque_plateau_abs) == (3, 5, 0.0, 0.0)
+
+
+class _Params:
+    def __init__(self, dt):
+        self.dt = dt
+
+
+def test_equilibrate_remanence_resets_dt(gpu):
+    s = _Scripted([_Rep(1e-4, 1e-3)])
+    p = _Params(3e-12)
+    out = E.equilibrate_remanence(s, p, 2, E.RemanencePolicy.default())
+    assert p.dt == 1e-13 and out.gate_passed and len(out.relax_passes) == 1
+
+
+def test_hysteresis_step_dt_and_premin(gpu):
+    """dt is reset on the first step or without warm start, kept otherwise; the optional
+    minimiser pass runs before the gated relax (equilibrate.rs:395-430)."""
+    pol = E.HysteresisPolicy.default()
+    s = _Scripted([_Rep(1e-4), _Rep(1e-4)])
+    p = _Params(3e-12)
+    rep = E.hysteresis_step(s, p, 2, pol, is_first=False)
+    assert p.dt == 3e-12 and rep.premin is None and rep.relax.gate_passed
+    rep = E.hysteresis_step(s, p, 2, pol, is_first=True)
+    assert p.dt == 1e-13
+    pol.premin = gpu.MinimizeSettings.default(max_iters=10)
+    pol.warm_start_dt = False
+    s = _Scripted([_Rep(1e-4)])
+    p = _Params(3e-12)
+    rep = E.hysteresis_step(s, p, 2, pol, is_first=False)
+    assert p.dt == 1e-13 and rep.premin == "mrep"
+    assert [c[0] for c in s.calls][:2] == ["minimize", "relax"]
