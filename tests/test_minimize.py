@@ -75,6 +75,15 @@ SCENARIOS = [
      dict(max_iters=5000), "converged"),
     ("anisotropy_exchange_only", dict(nx=32, ny=32, init="noise", seed=7, k_u=5e5), 0,
      dict(max_iters=3000), "max"),
+    # edge settings: a one-sample dM window from the first iteration, an immediate stall
+    ("dm_one_sample", dict(nx=16, ny=12, init="noise", seed=4), 2,
+     dict(max_iters=5000, torque_threshold=1e-9, dm_stop=1e-5, dm_samples=1, dm_min_iters=0), "dm"),
+    ("dm_samples_zero", dict(nx=16, ny=12, init="noise", seed=4), 2,
+     dict(max_iters=5000, torque_threshold=1e-9, dm_stop=1e-5, dm_samples=0, dm_min_iters=0), "dm"),
+    ("stall_immediately", dict(nx=16, ny=12, init="random", seed=4), 2,
+     dict(max_iters=100, dm_stop=None, stall_iters=0, min_iters_before_stall=0), "stalled"),
+    ("lambda_pinned", dict(nx=16, ny=12, init="noise", seed=4), 2,
+     dict(max_iters=2000, lambda0=1e-2, lambda_min=1e-2, lambda_max=1e-2), "converged"),
 ]
 
 
