@@ -45,16 +45,17 @@ def _fmt(v):
 
 
 def run_sp4(case="a", out_dir=None, precision=L.FP64, t_total=1e-9, dt_out=10e-12, dt_ovf=100e-12, device=0,
-            log=print):
+            log=print, solver=None):
     """Runs SP4 case 'a' or 'b'; returns a summary dict.  out_dir defaults to the
-    reference's runs/st_problems/sp4/sp4{a,b}_rust."""
+    reference's runs/st_problems/sp4/sp4{a,b}_rust.  `solver` replaces the GPU solver
+    of the 200x50 film (an object with the llg_b200.Solver methods used here)."""
     case = case.lower()
     b_ext = FIELDS.get(case, FIELDS["a"])
     if out_dir is None:
         out_dir = os.path.join("runs", "st_problems", "sp4", f"sp4{case if case in FIELDS else 'a'}_rust")
     os.makedirs(out_dir, exist_ok=True)
     grid, mat = sp4_setup()
-    s = L.Solver(grid, mat, precision, device=device)
+    s = solver if solver is not None else L.Solver(grid, mat, precision, device=device)
     m0 = np.array([1.0, 0.1, 0.0]) / math.sqrt(1.01)
     s.set_state(np.tile(m0, (grid.nx * grid.ny, 1)))
 
