@@ -2,6 +2,7 @@
 declares, reports errors through statuses, and its host-side input generators
 match the oracle bit for bit.  No GPU compute is called here."""
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -66,3 +67,35 @@ def test_demag_cache_filename_matches_reference_naming(gpu):
     g = gpu.Grid2D(2, 128, 1e-9, 1e-9, 0.5e-9)
     assert gpu.demag_cache_filename(g, 32, 0) == (
         "out/demag_cache/demag_kernel_nx2_ny128_pbcx32_pbcy0_px2_py256_dx1.000e-9_dy1.000e-9_dz5.000e-10_acc10.00.bin")
+
+
+def test_struct_layouts_match_header(gpu, tmp_path):
+    """Every public struct of include/llg_b200.h, as the C compiler lays it out, has the
+    size and field offsets of its ctypes mirror (the Rust #[repr(C)] structs of the
+    integration guide follow the same rules)."""
+    import subprocess
+
+    mirrors = {"llg_grid": gpu._Grid, "llg_material": gpu._Material, "llg_params": gpu._Params,
+               "llg_relax_settings": gpu.RelaxSettings, "llg_relax_report": gpu.RelaxReport,
+               "llg_minimize_settings": gpu.MinimizeSettings, "llg_minimize_report": gpu.MinimizeReport,
+               "llg_energy_breakdown": gpu.EnergyBreakdown, "llg_amr_patch": gpu._AmrPatch,
+               "llg_ovf_meta": gpu._OvfMeta}
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "llg_b200.h"', "int main(void) {"]
+    for cname, cls in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, key, val = line.split()
+        got[(cname, key)] = int(val)
+    for cname, cls in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
