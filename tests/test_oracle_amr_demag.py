@@ -174,3 +174,22 @@ def test_allfft_masks_and_samples(orc):
         for i in range(0, A.NX, 3):
             want = _py_sample(bf, 2 * A.NX, 2 * A.NY, A.DX / 2, A.DY / 2, (i + 0.5) * A.DX, (j + 0.5) * A.DY)
             assert list(bc[j * A.NX + i]) == want
+
+
+def test_benchmark_hierarchy_geometry(gpu):
+    """The benchmark's AMR workload: patches inside the 192x192 base, fine m of unit
+    vectors on each patch grid incl. ghosts, and the library's cell count per patch."""
+    import workloads as W
+
+    mc, patches = W.amr_vortex_hierarchy()
+    assert mc.shape == (192 * 192, 3)
+    assert np.allclose(np.linalg.norm(mc, axis=1), 1.0)
+    cover = np.zeros((192, 192), dtype=int)
+    for p in patches:
+        assert p.i0 >= 0 and p.j0 >= 0 and p.i0 + p.cnx <= 192 and p.j0 + p.cny <= 192
+        assert p.m.shape == (p.pnx * p.pny, 3) and np.allclose(np.linalg.norm(p.m, axis=1), 1.0)
+        gp = gpu.AmrPatch(p.i0, p.j0, p.cnx, p.cny, p.ratio, p.ghost, p.m)
+        assert gpu.lib().llg_amr_patch_cells(gpu.C.byref(gp._c())) == p.pnx * p.pny
+        cover[p.j0:p.j0 + p.cny, p.i0:p.i0 + p.cnx] = 1
+    assert 0.15 < cover.mean() < 0.17          # level-1 coverage of the quoted workload (~16 %)
+    assert sorted({p.ratio for p in patches}) == [2, 4, 8]
