@@ -115,74 +115,124 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline: the FP64 oracle (C++ restatement of the reference path)
 # ---------------------------------------------------------------------------
-def cpu_baseline(budget_s=20.0, warmup_steps=0):
+CPU_VARIANTS = {
+    "reference-threading": "demag FFT loops OpenMP-parallel on all threads, local terms / torques / RK "
+                           "combinations serial (the reference's rayon structure, demag_fft_uniform.rs:110-133)",
+    "fully-parallel": "demag FFT loops and the per-cell local-term / torque / RK-combination loops "
+                      "OpenMP-parallel on all threads",
+}
+
+
+def cpu_host_info():
+    """Threads available to this process and the CPU model."""
+    try:
+        aff = len(os.sched_getaffinity(0))
+    except AttributeError:
+        aff = os.cpu_count() or 1
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"threads": aff, "logical_cpus": os.cpu_count(), "cpu_model": model,
+            "omp_proc_bind": os.environ.get("OMP_PROC_BIND", "unset"), "omp_places": os.environ.get("OMP_PLACES", "unset")}
+
+
+def cpu_leg(variant, warmup_steps, max_steps, budget_s):
+    """Accepted FP64 RK45 steps of the benchmark film on the host cores: the oracle with
+    all threads this process may use, `variant` selecting the threading structure.
+    Returns (cell-steps/s, accepted, rejected, seconds, threads)."""
     import oracle as O
 
     w = WORKLOAD
-    threads = os.cpu_count() or 1
+    threads = cpu_host_info()["threads"]
     O.set_threads(threads)
-    n = w["nx"] * w["ny"]
-    g = O.make_grid(w["nx"], w["ny"], w["dx"], w["dy"], w["dz"])
-    mat = O.make_material(w["ms"], w["a_ex"], w["k_u"], w["easy"], w["dmi"], True)
-    s = O.Solver(g, mat)
-    m = O.init_random(n, w["seed"])
-    p = O.make_params(GAMMA, w["alpha"], w["dt0"], w["b_ext"])
-    s.build_h_eff(m, w["b_ext"], 2)  # builds the cached demag operator (untimed, as the reference caches it)
-    args = (2, w["max_err"], w["headroom"], w["dt_min"], w["dt_max"])
-    for _ in range(warmup_steps):
-        s.step_rk45(m, p, *args)
-    acc = rej = 0
-    t0 = time.perf_counter()
-    while True:
-        _, a, _ = s.step_rk45(m, p, *args)
-        acc += a
-        rej += not a
-        el = time.perf_counter() - t0
-        if acc >= 1 and el >= budget_s:
-            break
-    return {"value": n * acc / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{w['nx']}x{w['ny']} film of the same workload, FP64 oracle (C++ restatement, demag "
-                      f"FFT OpenMP-parallel, local terms serial as in the reference), {acc} accepted + {rej} "
-                      f"rejected RK45 steps in {el:.1f} s"}
-
-
-def run_reference(args):
-    world, rank, _ = dist_env()
-    if rank != 0:
-        return 0
-    budget = 90.0
-    import oracle as O
-
-    w = WORKLOAD
-    threads = os.cpu_count() or 1
-    O.set_threads(threads)
+    O.set_parallel_local(variant == "fully-parallel")
     n = w["nx"] * w["ny"]
     g = O.make_grid(w["nx"], w["ny"], w["dx"], w["dy"], w["dz"])
     s = O.Solver(g, O.make_material(w["ms"], w["a_ex"], w["k_u"], w["easy"], w["dmi"], True))
     m = O.init_random(n, w["seed"])
     p = O.make_params(GAMMA, w["alpha"], w["dt0"], w["b_ext"])
-    s.build_h_eff(m, w["b_ext"], 2)
+    s.build_h_eff(m, w["b_ext"], 2)  # builds the cached demag operator (untimed: the reference caches it)
     sargs = (2, w["max_err"], w["headroom"], w["dt_min"], w["dt_max"])
-    for _ in range(min(args.warmup, 1)):
+    for _ in range(warmup_steps):
         s.step_rk45(m, p, *sargs)
     acc = rej = 0
     t0 = time.perf_counter()
-    while acc < args.steps:
+    while acc < max_steps:
         _, a, _ = s.step_rk45(m, p, *sargs)
         acc += a
         rej += not a
-        if time.perf_counter() - t0 > budget and acc >= 1:
+        if acc >= 1 and time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
-    value = n * acc / el
+    return n * acc / el, acc, rej, el, threads
+
+
+def cpu_baseline_fresh(warmup_steps, max_steps, budget_s):
+    """Both CPU variants, each timed in a fresh process (no GPU context, no torch
+    threads, no sampler running), so the figure does not depend on what ran before."""
+    out = {}
+    for variant in CPU_VARIANTS:
+        cmd = [sys.executable, os.path.abspath(__file__), "--cpu-leg", variant, "--warmup", str(warmup_steps),
+               "--steps", str(max_steps), "--cpu-budget", str(budget_s)]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=budget_s * 3 + 300)
+        if r.returncode != 0:
+            out[variant] = {"error": r.stderr.strip().splitlines()[-1:] or ["failed"]}
+            continue
+        out[variant] = json.loads(r.stdout.strip().splitlines()[-1])
+    ref = out.get("reference-threading", {})
+    par = out.get("fully-parallel", {})
+    info = cpu_host_info()
+    if "value" not in ref:
+        return {"value": None, "unit": UNIT, "cores": info["threads"], "kind": "port", "sample": str(out)}
+    return {"value": ref["value"], "unit": UNIT, "cores": ref["threads"], "kind": "port",
+            "sample": f"{ref['accepted']} accepted (+{ref['rejected']} rejected) FP64 RK45 steps of the full "
+                      f"{WORKLOAD['nx']}x{WORKLOAD['ny']} film after {warmup_steps} warm-up steps, oracle C++ "
+                      f"restatement, {CPU_VARIANTS['reference-threading']}, fresh process",
+            "fully_parallel": {"value": par.get("value"), "accepted": par.get("accepted"),
+                               "note": CPU_VARIANTS["fully-parallel"]},
+            "host": info}
+
+
+def run_cpu_leg(args):
+    value, acc, rej, el, threads = cpu_leg(args.cpu_leg, args.warmup, args.steps, args.cpu_budget)
+    print(json.dumps({"value": value, "accepted": acc, "rejected": rej, "seconds": el, "threads": threads}))
+    return 0
+
+
+def config_dict(world):
+    """The `config` object of both arms (identical keys and values)."""
+    w = WORKLOAD
+    n = w["nx"] * w["ny"]
+    return {"workload": workload_desc(), "cells_per_gpu": n, "global_cells": n * world,
+            "parallelism": f"independent films, 1 per GPU x{world}",
+            "l2": "inputs larger than L2: ~190 MB per film working set (m, 7 torques, stage states, 25 MB "
+                  "spectrum, 16 MB kernel) vs 126 MB L2"}
+
+
+def run_reference(args):
+    """The reference arm: the reference's CPU path (the oracle restatement with the
+    reference's threading structure) on all host threads, same workload, same
+    warm-up and step counts as the GPU arm, each step a full-film accepted step."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    budget = 150.0
+    value, acc, rej, el, threads = cpu_leg("reference-threading", args.warmup, args.steps, budget)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
-            "steps": acc, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * el / acc, "higher_is_better": True,
+            "steps": acc, "warmup": args.warmup, "ms_per_step": 1e3 * el / acc, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_desc(), "cells": n, "precision": "fp64 (reference arithmetic)"},
+            "config": config_dict(world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{acc} accepted (+{rej} rejected) RK45 steps of the full film, bounded "
-                                       f"to ~{budget:.0f} s; oracle C++ restatement (the Rust reference cannot "
-                                       f"be compiled here)"},
+                             "sample": f"{acc} accepted (+{rej} rejected) FP64 RK45 steps of the full film after "
+                                       f"{args.warmup} warm-up steps (bounded to ~{budget:.0f} s); oracle C++ "
+                                       f"restatement (the Rust reference cannot be compiled here), "
+                                       f"{CPU_VARIANTS['reference-threading']}",
+                             "host": cpu_host_info()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -487,6 +537,42 @@ def reduce_over_ranks(dist, x, op, device):
     return float(t.item())
 
 
+def _r(x, nd=4):
+    """Round floats for the one-line record (3-4 significant digits)."""
+    if isinstance(x, float):
+        return float(f"{x:.{nd}g}")
+    if isinstance(x, dict):
+        return {k: _r(v, nd) for k, v in x.items()}
+    if isinstance(x, list):
+        return [_r(v, nd) for v in x]
+    return x
+
+
+def compact_legs(batch, flow, warm, amr, sp4r, mini):
+    """Short per-leg summaries for the bench line (the full records go to --detail)."""
+    out = {}
+    if batch:
+        out["batch_c3"] = _r({"value": batch["value"], "ms": batch["ms"], "accepted_mean": batch["accepted_mean"],
+                              "rejected": batch["rejected"]})
+    if flow:
+        out["flow_c1"] = _r({"fp64_relax_s": flow["fp64"]["relax_s"], "fp32_relax_s": flow["fp32"]["relax_s"],
+                             "fp64_run_s": flow["fp64"]["run_s"], "fp32_run_s": flow["fp32"]["run_s"],
+                             "mean_m_max_abs_diff": flow["mean_m_max_abs_diff"]})
+    if warm:
+        out["warm_start_c5"] = _r({k: warm[k] for k in warm if k not in ("workload", "weights", "films")})
+    if amr:
+        out["amr_demag"] = _r({"coarse_fft_ms": amr["coarse_fft_ms"], "allfft_ms": amr["allfft_ms"],
+                               "cpu_coarse_fft_ms": amr.get("cpu_coarse_fft_ms")})
+    if sp4r:
+        out["sp4"] = _r({"fp32_wall_s": sp4r["fp32"]["wall_s"], "fp64_wall_s": sp4r["fp64"]["wall_s"],
+                         "crossover_t_s": sp4r["fp32"]["crossover_t_s"]})
+    if mini:
+        out["minimize"] = _r({"fp32_ms_per_iter": mini["fp32"]["ms_per_iter"],
+                              "fp64_ms_per_iter": mini["fp64"]["ms_per_iter"],
+                              "fp32_hbm_frac": mini["fp32"]["hbm_frac"]})
+    return out
+
+
 def run_gpu(args):
     import torch
 
@@ -576,42 +662,62 @@ def run_gpu(args):
     roofline_step = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s", "frac": step_ach / peak,
                      "bytes_per_cell_step": BYTES_PER_CELL_STEP, "peak_source": peak_kind}
 
-    # end to end through the reference-facing call with host buffers
-    e2e = None
+    # end to end through the reference-facing calls with host buffers.  e2e: the
+    # drop-in binding of step(&mut m, ...) (llg.rs:795): every accepted step uploads
+    # the caller's AoS f64 m from pinned memory (llg_set_state), runs llg_step_rk45
+    # attempts (params in, eps / accepted / dt out) and reads m back (llg_get_state).
+    # e2e_resident: the state stays on the GPU between steps (set once, read once).
+    e2e = e2e_res = None
     if not args.no_e2e:
         host_m = torch.from_numpy(m0.copy()).pin_memory()
-        host_out = torch.empty_like(host_m).pin_memory()
-        s2 = make_solver(L, L.FP32)
-        s2.set_stream(stream.cuda_stream)
-        p2 = params(L)
-        s2.set_state_ptr(host_m.data_ptr())
-        s2.run_rk45(p2, fm, *ctl, n_accepted=args.warmup)  # warm the graphs
-        p2 = params(L)
+        state_bytes = n * 3 * 8   # AoS f64 m; per attempt 64 B of llg_params in, 32 B of results out
+
+        def timed(per_step_copies, k):
+            s2 = make_solver(L, L.FP32)
+            s2.set_stream(stream.cuda_stream)
+            host_m.copy_(torch.from_numpy(m0))
+            s2.set_state_ptr(host_m.data_ptr())
+            p2 = params(L)
+            s2.run_rk45(p2, fm, *ctl, n_accepted=args.warmup)  # graphs and clocks warm
+            s2.get_state_ptr(host_m.data_ptr())
+            p2 = params(L)
+            torch.cuda.synchronize()
+            barrier()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            f0.record(stream)
+            acc2 = calls = 0
+            if not per_step_copies:
+                s2.set_state_ptr(host_m.data_ptr())
+            while acc2 < k:
+                if per_step_copies:
+                    s2.set_state_ptr(host_m.data_ptr())
+                a = 0
+                while not a:
+                    _, a, _ = s2.step_rk45(p2, fm, *ctl)
+                    calls += 1
+                acc2 += 1
+                if per_step_copies:
+                    s2.get_state_ptr(host_m.data_ptr())
+            if not per_step_copies:
+                s2.get_state_ptr(host_m.data_ptr())
+            f1.record(stream)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+            s2.close()
+            ms_e = max_over_ranks(max(f0.elapsed_time(f1), wall * 1e3))
+            nsets = acc2 if per_step_copies else 1
+            return {"value": n * acc2 * world / (ms_e * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": (state_bytes * nsets + 64 * calls) / acc2,
+                    "d2h_bytes_per_step": (state_bytes * nsets + 32 * calls) / acc2, "steps": acc2,
+                    "attempts": calls, "ms_per_step": ms_e / acc2}
+
         k_e2e = max(1, min(args.steps, 100))
-        torch.cuda.synchronize()
-        barrier()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        t0 = time.perf_counter()
-        f0.record(stream)
-        s2.set_state_ptr(host_m.data_ptr())
-        acc2 = 0
-        calls = 0
-        while acc2 < k_e2e:
-            _, a, _ = s2.step_rk45(p2, fm, *ctl)
-            acc2 += a
-            calls += 1
-        s2.get_state_ptr(host_out.data_ptr())
-        f1.record(stream)
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        ms_e2e = max_over_ranks(max(f0.elapsed_time(f1), wall * 1e3))
-        state_bytes = n * 3 * 8
-        e2e = {"value": n * acc2 * world / (ms_e2e * 1e-3), "unit": UNIT,
-               "h2d_bytes_per_step": state_bytes / acc2, "d2h_bytes_per_step": (state_bytes + 192 * calls) / acc2,
-               "steps": acc2, "calls": calls,
-               "path": "llg_set_state (pinned AoS f64) + llg_step_rk45 per attempt (host params in, eps/accepted/"
-                       "dt out) + llg_get_state"}
-        s2.close()
+        e2e = timed(True, k_e2e)
+        e2e["path"] = ("per accepted step: llg_set_state (pinned AoS f64 m in) + llg_step_rk45 attempts + "
+                       "llg_get_state (m out), as a binding of step(&mut m, ...) does")
+        e2e_res = timed(False, k_e2e)
+        e2e_res["path"] = "llg_set_state once + llg_step_rk45 per attempt + llg_get_state once"
 
     # FP32 vs FP64 at matched simulated time from the same initial state
     fp64 = None
@@ -663,20 +769,22 @@ def run_gpu(args):
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.cpu_budget)
+        cpu = cpu_baseline_fresh(min(args.warmup, 2), args.steps, args.cpu_budget)
 
     if rank == 0:
+        cfg = config_dict(world)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": acc, "warmup": args.warmup,
                 "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_desc(), "cells_per_gpu": n, "global_cells": n * world,
-                           "parallelism": f"independent films, 1 per GPU x{world}", "rejected_steps": rej,
-                           "t_sim_s": t_adv,
-                           "l2": "inputs larger than L2: ~190 MB per film working set (m, 7 torques, stage states, "
-                                 "25 MB spectrum, 16 MB kernel) vs 126 MB L2"},
+                "dtype": "f32", "data": "synthetic", "config": cfg,
+                "rejected_steps": rej, "t_sim_s": t_adv,
                 "clocks": clk, "gpu_launches": launches, "roofline": roofline, "roofline_step": roofline_step,
-                "e2e": e2e, "fp64": fp64, "batch": batch, "flow": flow, "warm_start": warm, "amr_demag": amr, "sp4": sp4r, "minimize": mini,
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu, "e2e": e2e, "e2e_resident": e2e_res,
+                "legs": compact_legs(batch, flow, warm, amr, sp4r, mini),
+                "fp64": fp64}
+        if args.detail:
+            with open(args.detail, "w") as fh:
+                json.dump({"batch": batch, "flow": flow, "warm_start": warm, "amr_demag": amr, "sp4": sp4r,
+                           "minimize": mini, "line": line}, fh, indent=1)
         print(json.dumps(line), flush=True)
     s.close()
     if dist is not None:
@@ -694,7 +802,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--fp64-steps", type=int, default=2000)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-flow", action="store_true")
@@ -702,8 +810,12 @@ def main():
     ap.add_argument("--no-amr", action="store_true")
     ap.add_argument("--no-sp4", action="store_true")
     ap.add_argument("--no-minimize", action="store_true")
+    ap.add_argument("--detail", default=None, help="also write every leg's full record to this JSON file")
+    ap.add_argument("--cpu-leg", default=None, choices=sorted(CPU_VARIANTS), help=argparse.SUPPRESS)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.cpu_leg:
+        return run_cpu_leg(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)

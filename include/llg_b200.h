@@ -156,7 +156,11 @@ int llg_solver_destroy(llg_solver* s);
 int llg_solver_set_stream(llg_solver* s, void* stream);
 int llg_solver_sync(llg_solver* s);
 
-/* Upload / download the resident magnetisation (VectorField2D::data). */
+/* Upload / download the resident magnetisation (VectorField2D::data).
+ * An upload that equals the resident state bit for bit (the state just read
+ * back by llg_get_state) keeps the FSAL torque, so a binding that passes the
+ * caller's `&mut m` in and out of every step (llg.rs:795) steps exactly as a
+ * resident loop does; any other upload drops it. */
 int llg_set_state(llg_solver* s, const double* m_aos);
 int llg_get_state(llg_solver* s, double* m_aos);
 /* Mean magnetisation <m> of the resident state, FP64 reduction on the GPU. */
@@ -273,7 +277,9 @@ int llg_solver_launch_count(llg_solver* s, int64_t* out);
  * 24*(nx+1)*ny + 16*(nx+ny) <= 32 MiB (e.g. 1024 x 1024), else LLG_ERR_INVALID.
  * The first call on a device looks up the array's device address and opts the
  * kernels into large shared memory; make that first call before any stream
- * capture.  Every call shares the array (no state carries over: each call
+ * capture.  After cudaDeviceReset the next call on that device repeats this
+ * set-up (the reset drops the context the address belonged to), so it too
+ * belongs before any capture.  Every call shares the array (no state carries over: each call
  * rewrites all of it before reading), so calls that overlap on the GPU — on
  * different streams or from different threads — race; serialise them. */
 int llg_demag_field_noalloc(int64_t nx, int64_t ny, double ms, const float* m, const double* kernel_planes,

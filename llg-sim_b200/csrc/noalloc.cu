@@ -180,17 +180,26 @@ __global__ void __launch_bounds__(kThreads) k_na_rows_inverse(int nx, int ny, co
 }
 
 // Per-device set-up: device address of the static scratch (with the device
-// current) and the shared-memory opt-in of the three kernels.
+// current) and the shared-memory opt-in of the three kernels.  It runs on the
+// first call on a device, and again when the opt-in is gone (after
+// cudaDeviceReset the device has a new context: the static array is reloaded,
+// possibly at another address, and the kernels' attributes are back at their
+// defaults), so a cached address never outlives the context it came from.
 int setup(int dev, void** out) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
+    const int smax = 227 * 1024;
     if (g_scratch_addr[dev]) {
-        *out = g_scratch_addr[dev];
-        return LLG_OK;
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, k_na_rows_forward) == cudaSuccess && fa.maxDynamicSharedSizeBytes >= smax) {
+            *out = g_scratch_addr[dev];
+            return LLG_OK;
+        }
+        cudaGetLastError();
+        g_scratch_addr[dev] = nullptr;
     }
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
     if (e != cudaSuccess || !ptr) return LLG_ERR_CUDA;
-    const int smax = 227 * 1024;
     if (cudaFuncSetAttribute(k_na_rows_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, smax) != cudaSuccess ||
         cudaFuncSetAttribute(k_na_rows_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, smax) != cudaSuccess ||
         cudaFuncSetAttribute(k_na_column, cudaFuncAttributeMaxDynamicSharedMemorySize, smax) != cudaSuccess)

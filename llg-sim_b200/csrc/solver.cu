@@ -207,16 +207,30 @@ __global__ void k_mean_m(const FilmDev* films, const WorkItem* __restrict__ item
     }
 }
 
+__device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_uint(a) == __float_as_uint(b); }
+__device__ __forceinline__ bool same_bits(double a, double b) {
+    return __double_as_longlong(a) == __double_as_longlong(b);
+}
+
+// Uploaded AoS f64 state -> resident SoA planes.  The FSAL torque of the resident
+// state stays valid when the upload equals that state bit for bit (a caller that
+// passes back the state it just read, as a per-step host binding does); any
+// difference drops it (every thread that sees one writes the same 0).
 template <typename R>
 __global__ void k_aos_to_soa(const FilmDev* films, int film, const double* __restrict__ src) {
     const FilmDev& F = films[film];
     const int n = F.nx * F.ny;
     R* dst = mbuf<R>(F, MB_M0, F.st->cur);
+    bool changed = false;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
-        dst[idx] = (R)src[idx * 3 + 0];
-        dst[n + idx] = (R)src[idx * 3 + 1];
-        dst[2 * n + idx] = (R)src[idx * 3 + 2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const R v = (R)src[idx * 3 + c];
+            changed |= !same_bits(v, dst[c * n + idx]);
+            dst[c * n + idx] = v;
+        }
     }
+    if (__syncthreads_or(changed) && threadIdx.x == 0) F.st->fsal_valid = 0;
 }
 
 // The resident m as AoS f32 (the OVF binary4 payload), rounded to nearest.
@@ -744,10 +758,9 @@ struct Engine final : EngineBase {
         CUDA_TRY(cudaMemcpyAsync(d_stage, m, sizeof(double) * 3 * (size_t)cells(f), cudaMemcpyHostToDevice, stream));
         k_aos_to_soa<R><<<592, 256, 0, stream>>>(d_films, f, d_stage);
         CUDA_TRY(cudaGetLastError());
-        invalidate_fsal_host();
-        std::unique_ptr<bool[]> iv(new bool[nf]);
-        for (int e = 0; e < nf; ++e) iv[e] = e == f;
-        if ((rc = set_control(idle_control(), nullptr, iv.get(), true))) return rc;
+        launches += 1;
+        // FSAL validity of film f is decided on the device by k_aos_to_soa
+        if ((rc = set_control(idle_control(), nullptr, nullptr, true))) return rc;
         CUDA_TRY(cudaStreamSynchronize(stream));
         return LLG_OK;
     }

@@ -141,6 +141,11 @@ struct Fft1D {
 };
 
 int g_threads = 1;
+// Variant of the CPU baseline: the reference runs its local field terms, torques and
+// RK combinations serially on the caller (only the FFT demag uses rayon); with
+// g_par_local set those per-cell loops run OpenMP-parallel too.  Each cell's
+// arithmetic is unchanged, so results are identical in both modes.
+bool g_par_local = false;
 
 // fft2 over a px-by-py row-major array: rows then columns
 // (demag_fft_uniform.rs:777-922).  inverse scales by 1/(px*py) at the end.
@@ -421,6 +426,7 @@ void add_exchange(const orc_grid& g, const double* m, double* b, const orc_mater
     double coeff = 2.0 * a / ms;
     bool has_eta = mat.has_dmi && mat.dmi != 0.0;
     double eta = has_eta ? mat.dmi / (2.0 * a) : 0.0;
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_par_local)
     for (int64_t j = 0; j < ny; ++j) {
         for (int64_t i = 0; i < nx; ++i) {
             int64_t ic = j * nx + i;
@@ -471,6 +477,7 @@ void add_anisotropy(int64_t n, const double* m, double* b, const orc_material& m
     if (mat.k_u == 0.0 || mat.ms == 0.0) return;
     double coeff = 2.0 * mat.k_u / mat.ms;
     const double* u = mat.easy_axis;
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_par_local)
     for (int64_t i = 0; i < n; ++i) {
         const double* mc = &m[i * 3];
         double mdotu = mc[0] * u[0] + mc[1] * u[1] + mc[2] * u[2];
@@ -491,6 +498,7 @@ void add_dmi(const orc_grid& g, const double* m, double* b, const orc_material& 
     double pref = 2.0 * d / ms;
     double eta = d / (2.0 * a);
     auto inside = [&](int64_t idx) { return mask ? mask[idx] != 0 : true; };
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_par_local)
     for (int64_t j = 0; j < ny; ++j) {
         for (int64_t i = 0; i < nx; ++i) {
             int64_t ic = j * nx + i;
@@ -581,6 +589,7 @@ namespace {
 void build_h_eff(orc_solver* s, const double* m, const double* bext, int fmask, double* b) {
     int64_t n = s->n;
     const uint8_t* mask = s->maskp();
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_par_local)
     for (int64_t i = 0; i < n; ++i) {
         b[i * 3 + 0] = 0.0 + bext[0];
         b[i * 3 + 1] = 0.0 + bext[1];
@@ -606,6 +615,8 @@ extern "C" {
 
 void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
 int orc_get_threads(void) { return g_threads; }
+void orc_set_parallel_local(int on) { g_par_local = on != 0; }
+int orc_get_parallel_local(void) { return g_par_local ? 1 : 0; }
 
 orc_solver* orc_solver_create(const orc_grid* g, const orc_material* mat, const uint8_t* geom_mask) {
     orc_solver* s = new orc_solver();
@@ -672,10 +683,12 @@ void orc_step_rk45(orc_solver* s, double* m, orc_params* p, int fmask, double ma
         K[1] = K[7];
     } else {
         build_h_eff(s, m, p->b_ext, fmask, Bf[1].data());
+    #pragma omp parallel for schedule(static) num_threads(g_threads) if (g_par_local)
         for (int64_t i = 0; i < n; ++i) llg_rhs(&m[i * 3], &Bf[1][i * 3], gamma, alpha, &K[1][i * 3]);
     }
     // stage s: m_s = normalize(m + sum_j (dt0*a_sj) k_j), then B_s and k_s
     auto stage = [&](int st, int nk, const int* ks, const double* as) {
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_par_local)
         for (int64_t i = 0; i < n; ++i) {
             double v[3] = {m[i * 3], m[i * 3 + 1], m[i * 3 + 2]};
             for (int q = 0; q < nk; ++q) {
@@ -688,6 +701,7 @@ void orc_step_rk45(orc_solver* s, double* m, orc_params* p, int fmask, double ma
             stage_normalize(s, i, v, &M[st][i * 3]);
         }
         build_h_eff(s, M[st].data(), p->b_ext, fmask, Bf[st].data());
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_par_local)
         for (int64_t i = 0; i < n; ++i) llg_rhs(&M[st][i * 3], &Bf[st][i * 3], gamma, alpha, &K[st][i * 3]);
     };
     {
@@ -721,6 +735,7 @@ void orc_step_rk45(orc_solver* s, double* m, orc_params* p, int fmask, double ma
         stage(7, 5, ks, as);
     }
     double err_inf = 0.0;
+#pragma omp parallel for schedule(static) num_threads(g_threads) if (g_par_local) reduction(max : err_inf)
     for (int64_t i = 0; i < n; ++i) {
         double d = 0.0;
         for (int c = 0; c < 3; ++c) {

@@ -110,6 +110,10 @@ typedef struct orc_solver orc_solver;
 
 void orc_set_threads(int n);
 int orc_get_threads(void);
+// 1: also run the per-cell local-term, torque and RK-combination loops in parallel
+// (the reference runs them serially); results are identical either way.
+void orc_set_parallel_local(int on);
+int orc_get_parallel_local(void);
 
 /* geom_mask: nullable; one byte per cell, nonzero = material. */
 orc_solver* orc_solver_create(const orc_grid* g, const orc_material* mat, const uint8_t* geom_mask);

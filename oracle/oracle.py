@@ -132,6 +132,8 @@ def lib():
         L.orc_init_uniform_with_noise.argtypes = [C.c_int64, dp, C.c_double, C.c_uint64, dp]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
+        L.orc_set_parallel_local.argtypes = [C.c_int]
+        L.orc_get_parallel_local.restype = C.c_int
         _lib = L
     return _lib
 
@@ -150,6 +152,16 @@ def set_threads(n):
 
 def get_threads():
     return lib().orc_get_threads()
+
+
+def set_parallel_local(on):
+    """Also parallelise the per-cell local-term, torque and RK-combination loops
+    (the reference runs them serially); results are identical either way."""
+    lib().orc_set_parallel_local(1 if on else 0)
+
+
+def get_parallel_local():
+    return bool(lib().orc_get_parallel_local())
 
 
 def make_grid(nx, ny, dx, dy, dz):
