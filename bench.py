@@ -631,17 +631,27 @@ def run_gpu(args):
     step_ms = ms / acc
     peak, peak_kind = peaks()
 
-    # per-kernel roofline of one RK45 stage (same state, CUDA events per pass)
+    # per-kernel roofline of one RK45 stage (same state, CUDA events per pass).  An
+    # accepted FSAL step launches the row-forward pass once (stage 2), the column
+    # pass six times, the fused row pass five times (stages 2->3 .. 6->7) and the
+    # row-inverse pass once (stage 7, with the error norm); the dominant kernel is
+    # the one with the largest share of the step's device time.
     prof = s.profile_stage(p, fm, reps=30)
     K1 = w["nx"] + 1
     x_bytes = 3 * K1 * w["ny"] * 8
     khat_bytes = K1 * (w["ny"] + 1) * 16
     plane = 3 * n * 4
-    bytes_pass = {"k_row_forward": plane * (1 + 3 + 1) + x_bytes,   # m0 + 3 torques + m_s out + X out
-                  "k_column": 2 * x_bytes + khat_bytes,            # X in/out + kernel planes
-                  "k_row_inverse": x_bytes + 2 * plane}            # X in + m_s in + k out
-    names = ["k_row_forward", "k_column", "k_row_inverse"]
-    dom = names[int(np.argmax(prof))]
+    names = ["k_row_forward", "k_column", "k_row_inverse", "k_row_fused"]
+    bytes_pass = {"k_row_forward": plane * (1 + 3 + 1) + x_bytes,      # m0 + 3 torques + m_s out + X out
+                  "k_column": 2 * x_bytes + khat_bytes,               # X in/out + kernel planes
+                  "k_row_inverse": x_bytes + 2 * plane,               # X in + m_s in + k out
+                  "k_row_fused": 2 * x_bytes + plane * (1 + 1 + 1 + 3 + 1)}   # X in/out, m_s, k_s, m0, 3 k, m_next
+    per_step = {"k_row_forward": 1, "k_column": 6, "k_row_inverse": 1, "k_row_fused": 5}
+    if prof[3] <= 0.0:   # no fused pass on this path: every stage runs the three passes
+        per_step = {"k_row_forward": 6, "k_column": 6, "k_row_inverse": 6, "k_row_fused": 0}
+    live = [k for k in names if per_step[k] > 0]
+    share = {k: per_step[k] * float(prof[names.index(k)]) for k in live}
+    dom = max(live, key=lambda k: share[k])
     dom_ms = float(prof[names.index(dom)])
     achieved = bytes_pass[dom] / (dom_ms * 1e-3) / 1e9
     traffic = None
@@ -656,8 +666,10 @@ def run_gpu(args):
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "bytes_per_launch": bytes_pass[dom], "ms_per_launch": dom_ms,
-                "per_pass_ms": {k: float(v) for k, v in zip(names, prof)},
-                "per_pass_frac": {k: bytes_pass[k] / (float(v) * 1e-3) / 1e9 / peak for k, v in zip(names, prof)}}
+                "launches_per_step": {k: per_step[k] for k in live},
+                "per_pass_ms": {k: _r(float(prof[names.index(k)])) for k in live},
+                "per_pass_frac": {k: _r(bytes_pass[k] / (float(prof[names.index(k)]) * 1e-3) / 1e9 / peak)
+                                  for k in live}}
     step_ach = BYTES_PER_CELL_STEP * n * acc / (ms_local * 1e-3) / 1e9
     roofline_step = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s", "frac": step_ach / peak,
                      "bytes_per_cell_step": BYTES_PER_CELL_STEP, "peak_source": peak_kind}

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define LLG_B200_ABI_VERSION 1
+#define LLG_B200_ABI_VERSION 2
 
 enum llg_status {
     LLG_OK = 0,
@@ -253,11 +253,12 @@ int llg_batch_compute_energy(llg_batch* b, const double* b_ext /* 3*nfilms */, l
 int llg_batch_launch_count(llg_batch* b, int64_t* out);
 
 /* ---------------- instrumentation (no reference counterpart) ----------------
- * llg_profile_stage: CUDA-event timing of the three passes of one RK45 stage
- * evaluation (row forward, column, row inverse), averaged over `reps`
- * launches on the solver stream; ms3 receives milliseconds per pass.
+ * llg_profile_stage: CUDA-event timing of the passes of one RK45 stage
+ * evaluation, averaged over `reps` launches on the solver stream; ms4 receives
+ * milliseconds per pass: row forward, column, row inverse, and the fused row
+ * pass that ends this stage and starts the next (0 when no film uses it).
  * llg_solver_launch_count: kernels this solver has issued so far. */
-int llg_profile_stage(llg_solver* s, const llg_params* params, int32_t field_mask, int32_t reps, double* ms3);
+int llg_profile_stage(llg_solver* s, const llg_params* params, int32_t field_mask, int32_t reps, double* ms4);
 int llg_solver_launch_count(llg_solver* s, int64_t* out);
 
 /* ---------------- demag field without device allocation ----------------

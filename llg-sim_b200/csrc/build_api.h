@@ -47,7 +47,10 @@ struct LaunchGeom {
     int grid_rinv;    // register-FFT row-inverse pass, lean epilogue
     int grid_rfull;   // register-FFT row-inverse pass, full epilogue
     int grid_col;
+    int grid_fused;   // fused row pass (k_row_fused)
     bool any_demag;
+    bool fuse_rows;   // end a stage and start the next in one row pass where possible
+    bool col_direct;  // column pass loads its spectrum straight into registers
     int fast_row;     // register-FFT row kernels for L = nx (0: generic kernels)
     int fast_col;     // register-FFT column kernel for L = ny (0: generic kernel)
     int row_threads;
@@ -67,8 +70,15 @@ template <typename R>
 FastCfg fast_config(int nx, int ny);
 // Resident blocks per SM of the fast kernels (after prepare_eval_kernels).
 template <typename R>
-void fast_occupancy(int nx, int ny, int* fwd_blocks_per_sm, int* inv_blocks_per_sm, int* full_blocks_per_sm,
-                    int* col_blocks_per_sm);
+void fast_occupancy(int nx, int ny, bool col_direct, int* fwd_blocks_per_sm, int* inv_blocks_per_sm,
+                    int* full_blocks_per_sm, int* fused_blocks_per_sm, int* col_blocks_per_sm);
+// Whether stage si's row inverse and stage sf's row forward can run as one fused
+// row pass on segment g (register-FFT rows, lean epilogue, sf's combination ends
+// with si's torque).
+bool can_fuse(const EvalSpec& si, const EvalSpec& sf, const LaunchGeom& g);
+template <typename R>
+cudaError_t launch_fused(const EvalSpec& si, const EvalSpec& sf, const LaunchGeom& g, cudaStream_t s,
+                         int* nk = nullptr);
 template <typename R>
 cudaError_t build_pass_tables(void* out_row, int nx, void* out_col, int ny, cudaStream_t s);
 

@@ -3,6 +3,7 @@
 // shared-memory Stockham kernels otherwise.
 #include "build_api.h"
 #include "fast_kernels.cuh"
+#include "fused_kernels.cuh"
 #include "stage_kernels.cuh"
 
 #include <algorithm>
@@ -114,9 +115,19 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
             cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)RowCfg<R, L>::SMEM);
         }
+        if (RowCfg<R, L>::SMEM <= kSmemMax) {
+            cudaFuncSetAttribute(k_row_fused<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)RowCfg<R, L>::SMEM);
+            cudaFuncSetAttribute(k_row_fused<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        }
         if (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
             cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ColCfg<R, L>::SMEM);
+        if (ColDirectCfg<R, L>::SMEM <= kSmemMax) {
+            cudaFuncSetAttribute(k_column_direct<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ColDirectCfg<R, L>::SMEM);
+            cudaFuncSetAttribute(k_column_direct<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        }
         // the whole unified L1/shared array as shared memory, so that occupancy is
         // bounded by registers and the blocks' own shared memory only
         cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -182,9 +193,14 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
         if (g.fast_col) {
             dispatch_L<R>(g.fast_col, [&](auto LC) {
                 constexpr int L = decltype(LC)::value;
-                if constexpr (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
+                if (g.col_direct) {
+                    if constexpr (ColDirectCfg<R, L>::SMEM <= kSmemMax)
+                        k_column_direct<R, L><<<g.grid_col, ColCfg<R, L>::THREADS, ColDirectCfg<R, L>::SMEM, s>>>(
+                            g.films, g.col_items, g.n_col_items, spec);
+                } else if constexpr (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax) {
                     k_column_fast<R, L><<<g.grid_col, ColCfg<R, L>::THREADS, ColCfg<R, L>::SMEM, s>>>(
                         g.films, g.col_items, g.n_col_items, spec);
+                }
             });
         } else {
             k_column<R><<<g.grid_col, 256, g.smem_col, s>>>(g.films, g.col_items, g.n_col_items, spec);
@@ -192,6 +208,25 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
         ++count;
     }
     if (nk) *nk += count;
+    return cudaGetLastError();
+}
+
+bool can_fuse(const EvalSpec& si, const EvalSpec& sf, const LaunchGeom& g) {
+    return g.fast_row != 0 && g.fuse_rows && lean_epilogue(si) && si.k_out != KB_NONE && !si.skip_if_fsal &&
+           !sf.skip_if_fsal && sf.nterm >= 1 && sf.nterm <= 6 && sf.kidx[sf.nterm - 1] == si.k_out &&
+           sf.req == si.req && sf.demag == si.demag && sf.m_in != si.m_in;
+}
+
+template <typename R>
+cudaError_t launch_fused(const EvalSpec& si, const EvalSpec& sf, const LaunchGeom& g, cudaStream_t s, int* nk) {
+    dispatch_L<R>(g.fast_row, [&](auto LC) {
+        constexpr int L = decltype(LC)::value;
+        if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
+            using C = RowCfg<R, L>;
+            k_row_fused<R, L><<<g.grid_fused, C::THREADS, C::SMEM, s>>>(g.films, g.row_items, g.n_row_items, si, sf);
+        }
+    });
+    if (nk) *nk += 1;
     return cudaGetLastError();
 }
 
@@ -207,9 +242,9 @@ cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t 
 }
 
 template <typename R>
-void fast_occupancy(int nx, int ny, int* fwd_blocks_per_sm, int* inv_blocks_per_sm, int* full_blocks_per_sm,
-                    int* col_blocks_per_sm) {
-    *fwd_blocks_per_sm = *inv_blocks_per_sm = *full_blocks_per_sm = *col_blocks_per_sm = 1;
+void fast_occupancy(int nx, int ny, bool col_direct, int* fwd_blocks_per_sm, int* inv_blocks_per_sm,
+                    int* full_blocks_per_sm, int* fused_blocks_per_sm, int* col_blocks_per_sm) {
+    *fwd_blocks_per_sm = *inv_blocks_per_sm = *full_blocks_per_sm = *fused_blocks_per_sm = *col_blocks_per_sm = 1;
     dispatch_L<R>(nx, [&](auto LC) {
         constexpr int L = decltype(LC)::value;
         if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
@@ -223,20 +258,30 @@ void fast_occupancy(int nx, int ny, int* fwd_blocks_per_sm, int* inv_blocks_per_
             *fwd_blocks_per_sm = std::max(1, a);
             *inv_blocks_per_sm = std::max(1, b);
             *full_blocks_per_sm = std::max(1, c);
+            int d = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_row_fused<R, L>, RowCfg<R, L>::THREADS,
+                                                          RowCfg<R, L>::SMEM);
+            *fused_blocks_per_sm = std::max(1, d);
         }
     });
     dispatch_L<R>(ny, [&](auto LC) {
         constexpr int L = decltype(LC)::value;
         if constexpr (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax) {
             int a = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L>, ColCfg<R, L>::THREADS,
-                                                          ColCfg<R, L>::SMEM);
+            if (col_direct)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_direct<R, L>, ColCfg<R, L>::THREADS,
+                                                              ColDirectCfg<R, L>::SMEM);
+            else
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L>, ColCfg<R, L>::THREADS,
+                                                              ColCfg<R, L>::SMEM);
             *col_blocks_per_sm = std::max(1, a);
         }
     });
 }
-template void fast_occupancy<float>(int, int, int*, int*, int*, int*);
-template void fast_occupancy<double>(int, int, int*, int*, int*, int*);
+template void fast_occupancy<float>(int, int, bool, int*, int*, int*, int*, int*);
+template void fast_occupancy<double>(int, int, bool, int*, int*, int*, int*, int*);
+template cudaError_t launch_fused<float>(const EvalSpec&, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
+template cudaError_t launch_fused<double>(const EvalSpec&, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
 template FastCfg fast_config<float>(int, int);
 template FastCfg fast_config<double>(int, int);
 template cudaError_t build_pass_tables<float>(void*, int, void*, int, cudaStream_t);

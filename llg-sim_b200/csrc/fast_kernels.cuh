@@ -400,6 +400,108 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
 }
 
 // ---------------------------------------------------------------------------
+// Column pass without staging: the same transforms and kernel product as
+// k_column_fast, but each thread loads its E spectrum values straight from HBM /
+// L2 into registers (all loads of an item in flight at once, coalesced across the
+// transform group) and the kernel planes through L1.  Without the 40 KB staging
+// area three blocks fit per SM instead of two.
+template <typename R, int L>
+struct ColDirectCfg {
+    using C = ColCfg<R, L>;
+    static constexpr size_t SMEM = C::OFF_XST;
+};
+
+template <typename R, int L>
+__global__ void __launch_bounds__(ColCfg<R, L>::THREADS, (sizeof(R) == 4 && ColCfg<R, L>::THREADS <= 192) ? 3 : 1)
+    k_column_direct(const FilmDev* __restrict__ films,
+                                                                         const WorkItem* __restrict__ items,
+                                                                         int nitems, EvalSpec spec) {
+    using C = ColCfg<R, L>;
+    using FF = GroupFFT<R, L, false>;
+    using FI = GroupFFT<R, L, true>;
+    constexpr int G = C::G, E = C::E, BUF = C::BUF, NC = C::NC;
+    constexpr int ny = L, L2 = 2 * L;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<R>* buf = reinterpret_cast<cx<R>*>(smem_raw);
+    cx<R>* twp = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_TW);
+    cx<R>* pre = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_PRE);
+    const int tid = threadIdx.x, s = tid / G, t = tid % G;
+    const int cl = s / 6, comp = (s % 6) >> 1, par = s & 1;
+    bool tables = false;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const WorkItem w = items[it];
+        const FilmDev& F = films[w.film];
+        if (!(spec.demag && F.demag_mat) || skip_item(spec, F.st)) continue;   // uniform over the block
+        if (!tables) {
+            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_col), TwTab<R, L>::size, pre,
+                           reinterpret_cast<const cx<R>*>(F.tw_col), L);
+            tables = true;
+            __syncthreads();
+        }
+        const int K1 = F.nx + 1;
+        const int kx = w.blk * NC + cl;
+        const bool valid = kx < K1;
+        cx<R>* __restrict__ X = reinterpret_cast<cx<R>*>(F.X);
+        const cx<R>* __restrict__ col = X + ((size_t)comp * K1 + (valid ? kx : 0)) * ny;
+        cx<R> v[E];
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = valid ? col[t + G * r] : mkc((R)0, (R)0);
+#pragma unroll
+        for (int r = 0; r < E; ++r)
+            if (par) v[r] = cmul(v[r], pre[t + G * r]);
+        FF::run(v, t, buf + s * BUF, twp);
+        group_sync<G>();
+#pragma unroll
+        for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FF::out_index(t, i))] = v[i];
+        __syncthreads();   // all components of the column transformed
+        const r4<R>* __restrict__ kc = reinterpret_cast<const r4<R>*>(F.Khat) + (size_t)(valid ? kx : 0) * (L + 1);
+        const cx<R>* sx = buf + (6 * cl + 0 + par) * BUF;
+        const cx<R>* sy = buf + (6 * cl + 2 + par) * BUF;
+        const cx<R>* sz = buf + (6 * cl + 4 + par) * BUF;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const int kk = t + G * r;
+            const int ky = 2 * kk + par;
+            // the kernel spectrum is even in ky except Kxy, which is odd
+            const bool up = ky > ny;
+            const r4<R> K = kc[up ? L2 - ky : ky];
+            const R kxy = up ? -K.y : K.y;
+            const int pi = padi<E>(kk);
+            cx<R> out;
+            if (comp == 0) {
+                const cx<R> Mx = sx[pi], My = sy[pi];
+                out = mkc(K.x * Mx.re + kxy * My.re, K.x * Mx.im + kxy * My.im);
+            } else if (comp == 1) {
+                const cx<R> Mx = sx[pi], My = sy[pi];
+                out = mkc(kxy * Mx.re + K.z * My.re, kxy * Mx.im + K.z * My.im);
+            } else {
+                const cx<R> Mz = sz[pi];
+                out = mkc(K.w * Mz.re, K.w * Mz.im);
+            }
+            v[r] = out;
+        }
+        __syncthreads();   // products formed: the signal buffers are free
+        FI::run(v, t, buf + s * BUF, twp);
+        group_sync<G>();
+        if (par) {
+#pragma unroll
+            for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FI::out_index(t, i))] = v[i];
+        }
+        __syncthreads();   // odd-bin results visible to the even-bin groups
+        if (!par && valid) {
+            const cx<R>* ob = buf + (s + 1) * BUF;
+            cx<R>* __restrict__ dst = X + ((size_t)comp * K1 + kx) * ny;
+#pragma unroll
+            for (int i = 0; i < E; ++i) {
+                const int nn = FI::out_index(t, i);
+                dst[nn] = v[i] + cmulc(ob[padi<E>(nn)], pre[nn]);
+            }
+        }
+        __syncthreads();   // buffers reused by the next item
+    }
+}
+
+// ---------------------------------------------------------------------------
 // MODE 0: full epilogue; 1: no epilogue, the demag field is written to the film's
 // bdem planes for k_stage_torque; 2: the minimiser epilogue (RHS_MINIMIZE).
 template <typename R, int L, int MODE>

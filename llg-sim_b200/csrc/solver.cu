@@ -284,17 +284,18 @@ struct EngineBase {
     virtual int energy(const double* bext3n, llg_energy_breakdown* out) = 0;
     virtual int torque_metric(const llg_params* p, int fmask, int metric, double* out) = 0;
     virtual int kernel_kspace(int f, double* out) = 0;
-    virtual int profile_stage(const llg_params* p, int fmask, int reps, double* ms3) = 0;
+    virtual int profile_stage(const llg_params* p, int fmask, int reps, double* ms4) = 0;
     virtual long long launch_count() = 0;
     virtual int warm_start(ws::Net* net, const double* bext3n) = 0;
 };
 
 // LLG_B200_GENERIC_FFT=1 selects the generic shared-memory Stockham kernels
 // even where a register-FFT kernel exists (used to cross-check the two paths).
-static bool force_generic() {
-    const char* e = std::getenv("LLG_B200_GENERIC_FFT");
+static bool env_flag(const char* name) {
+    const char* e = std::getenv(name);
     return e && e[0] == '1';
 }
+static bool force_generic() { return env_flag("LLG_B200_GENERIC_FFT"); }
 
 template <typename R>
 struct Engine final : EngineBase {
@@ -337,7 +338,7 @@ struct Engine final : EngineBase {
     // launch segments: films grouped by the row (rseg) / column (cseg) kernel they use,
     // with the resident blocks per SM of each segment's kernels
     std::vector<LaunchGeom> rseg, cseg;
-    std::vector<std::array<int, 3>> rocc;
+    std::vector<std::array<int, 4>> rocc;
     std::vector<int> cocc;
 
     int nfilms() const override { return nf; }
@@ -372,6 +373,33 @@ struct Engine final : EngineBase {
         if (e.demag && geom.any_demag)
             for (auto& sg : cseg) CUDA_TRY(launch_one<R>(1, e, sg, stream, &nk));
         for (auto& sg : rseg) CUDA_TRY(launch_one<R>(2, e, sg, stream, &nk));
+        launches += nk;
+        return LLG_OK;
+    }
+
+    // The stages of one attempt in order.  Where a segment allows it (register-FFT
+    // rows, a lean stage followed by a combination that ends with its torque),
+    // stage i's row inverse and stage i+1's row forward run as one fused row pass.
+    int eval_chain(const std::vector<EvalSpec>& v) {
+        int nk = 0;
+        const int n = (int)v.size();
+        std::vector<char> fwd_done(rseg.size(), 0);
+        for (int i = 0; i < n; ++i) {
+            const EvalSpec& e = v[i];
+            for (size_t q = 0; q < rseg.size(); ++q)
+                if (!fwd_done[q]) CUDA_TRY(launch_one<R>(0, e, rseg[q], stream, &nk));
+            if (e.demag && geom.any_demag)
+                for (auto& sg : cseg) CUDA_TRY(launch_one<R>(1, e, sg, stream, &nk));
+            for (size_t q = 0; q < rseg.size(); ++q) {
+                if (i + 1 < n && can_fuse(e, v[i + 1], rseg[q])) {
+                    CUDA_TRY(launch_fused<R>(e, v[i + 1], rseg[q], stream, &nk));
+                    fwd_done[q] = 1;
+                } else {
+                    CUDA_TRY(launch_one<R>(2, e, rseg[q], stream, &nk));
+                    fwd_done[q] = 0;
+                }
+            }
+        }
         launches += nk;
         return LLG_OK;
     }
@@ -548,6 +576,8 @@ struct Engine final : EngineBase {
         geom.any_demag = any_demag;
         geom.fast_row = 0;
         geom.fast_col = 0;
+        geom.fuse_rows = !env_flag("LLG_B200_NO_FUSE");
+        geom.col_direct = !env_flag("LLG_B200_COL_STAGED");
         CUDA_TRY(prepare_eval_kernels<R>(smem_row, smem_col));
         {
             // persistent grids: at most one wave of resident blocks looping over the work
@@ -566,21 +596,22 @@ struct Engine final : EngineBase {
                 s.row_items = d_row_items + sp.second.first;
                 s.n_row_items = (int)sp.second.second;
                 s.fast_row = sp.first;
-                int fb = gen_r, ib = gen_r, ub = gen_r, cb = 1;
-                if (sp.first) fast_occupancy<R>(sp.first, 0, &fb, &ib, &ub, &cb);
+                int fb = gen_r, ib = gen_r, ub = gen_r, zb = 1, cb = 1;
+                if (sp.first) fast_occupancy<R>(sp.first, 0, geom.col_direct, &fb, &ib, &ub, &zb, &cb);
                 s.grid_row = balanced(s.n_row_items, fb);
                 s.grid_rinv = balanced(s.n_row_items, ib);
                 s.grid_rfull = balanced(s.n_row_items, ub);
+                s.grid_fused = balanced(s.n_row_items, zb);
                 rseg.push_back(s);
-                rocc.push_back({fb, ib, ub});
+                rocc.push_back({fb, ib, ub, zb});
             }
             for (auto& sp : cspan) {
                 LaunchGeom s = geom;
                 s.col_items = d_col_items + sp.second.first;
                 s.n_col_items = (int)sp.second.second;
                 s.fast_col = sp.first;
-                int fb = 1, ib = 1, ub = 1, cb = gen_c;
-                if (sp.first) fast_occupancy<R>(0, sp.first, &fb, &ib, &ub, &cb);
+                int fb = 1, ib = 1, ub = 1, zb = 1, cb = gen_c;
+                if (sp.first) fast_occupancy<R>(0, sp.first, geom.col_direct, &fb, &ib, &ub, &zb, &cb);
                 s.grid_col = balanced(s.n_col_items, cb);
                 cseg.push_back(s);
                 cocc.push_back(cb);
@@ -614,6 +645,9 @@ struct Engine final : EngineBase {
         stage.k_out = KB_K4;
         EvalSpec full = stage;
         full.reduce = 1;
+        EvalSpec next = stage;   // the stage after `stage`, for the fused row pass
+        combo(next, MB_S1, {KB_K1, KB_K2, KB_K3, KB_K4}, {dp5::A51, dp5::A52, dp5::A53, dp5::A54});
+        next.k_out = KB_K5;
         cudaEvent_t e0, e1;
         CUDA_TRY(cudaEventCreate(&e0));
         CUDA_TRY(cudaEventCreate(&e1));
@@ -632,11 +666,14 @@ struct Engine final : EngineBase {
         auto tune = [&](int which, const EvalSpec& spec, LaunchGeom& geom, int* grid, int items, int occ) -> int {
             float best = 1e30f;
             int best_g = *grid;
+            auto one = [&]() {
+                return which == 3 ? launch_fused<R>(spec, next, geom, stream) : launch_one<R>(which, spec, geom, stream);
+            };
             for (int g : candidates(items, occ)) {
                 *grid = g;
-                for (int w = 0; w < 2; ++w) CUDA_TRY(launch_one<R>(which, spec, geom, stream));
+                for (int w = 0; w < 2; ++w) CUDA_TRY(one());
                 CUDA_TRY(cudaEventRecord(e0, stream));
-                for (int r = 0; r < 4; ++r) CUDA_TRY(launch_one<R>(which, spec, geom, stream));
+                for (int r = 0; r < 4; ++r) CUDA_TRY(one());
                 CUDA_TRY(cudaEventRecord(e1, stream));
                 CUDA_TRY(cudaEventSynchronize(e1));
                 float ms = 0.f;
@@ -655,6 +692,7 @@ struct Engine final : EngineBase {
             if ((rc = tune(0, stage, sg, &sg.grid_row, nr, rocc[i][0]))) return rc;
             if ((rc = tune(2, stage, sg, &sg.grid_rinv, nr, rocc[i][1]))) return rc;
             if ((rc = tune(2, full, sg, &sg.grid_rfull, nr, rocc[i][2]))) return rc;
+            if (sg.fast_row && sg.fuse_rows && (rc = tune(3, stage, sg, &sg.grid_fused, nr, rocc[i][3]))) return rc;
         }
         for (size_t i = 0; i < cseg.size(); ++i)
             if ((rc = tune(1, stage, cseg[i], &cseg[i].grid_col, cseg[i].n_col_items, cocc[i]))) return rc;
@@ -873,30 +911,31 @@ struct Engine final : EngineBase {
     // One integrator attempt; req gates every kernel on StepState::req (relax).
     int launch_attempt(int kind, int fmask, int req) {
         int rc;
+        std::vector<EvalSpec> ch;
         EvalSpec e = base_spec(fmask);
         e.req = req;
         e.rhs = kind == KIND_RK45 ? RHS_LLG : RHS_RELAX;
         e.k_out = KB_K1;
         e.skip_if_fsal = 1;
-        if ((rc = eval(e))) return rc;
+        ch.push_back(e);
         e.skip_if_fsal = 0;
         if (kind == KIND_RK45) {
             using namespace dp5;
             combo(e, MB_S0, {KB_K1}, {A21});
             e.k_out = KB_K2;
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
             combo(e, MB_S1, {KB_K1, KB_K2}, {A31, A32});
             e.k_out = KB_K3;
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
             combo(e, MB_S0, {KB_K1, KB_K2, KB_K3}, {A41, A42, A43});
             e.k_out = KB_K4;
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
             combo(e, MB_S1, {KB_K1, KB_K2, KB_K3, KB_K4}, {A51, A52, A53, A54});
             e.k_out = KB_K5;
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
             combo(e, MB_S0, {KB_K1, KB_K2, KB_K3, KB_K4, KB_K5}, {A61, A62, A63, A64, A65});
             e.k_out = KB_K6;
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
             combo(e, MB_M7, {KB_K1, KB_K3, KB_K4, KB_K5, KB_K6}, {B1, B3, B4, B5, B6});
             e.k_out = KB_K7;
             e.err = ERR_RK45;
@@ -904,7 +943,8 @@ struct Engine final : EngineBase {
             const double wh[8] = {0, BH1, 0, BH3, BH4, BH5, BH6, BH7};
             std::memcpy(e.wb, wb, sizeof(wb));
             std::memcpy(e.wh, wh, sizeof(wh));
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
+            if ((rc = eval_chain(ch))) return rc;
             k_controller<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, 5, req);
             CUDA_TRY(cudaGetLastError());
             launches += 1;
@@ -912,10 +952,10 @@ struct Engine final : EngineBase {
             using namespace bs3;
             combo(e, MB_S0, {KB_K1}, {A21});
             e.k_out = KB_K2;
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
             combo(e, MB_S1, {KB_K2}, {A32});
             e.k_out = KB_K3;
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
             combo(e, MB_M7, {KB_K1, KB_K2, KB_K3}, {B1, B2, B3});
             e.k_out = KB_K7;
             e.err = ERR_RK23;
@@ -924,7 +964,8 @@ struct Engine final : EngineBase {
             const double wh[8] = {0, BH1, BH2, BH3, BH4, 0, 0, 0};
             std::memcpy(e.wb, wb, sizeof(wb));
             std::memcpy(e.wh, wh, sizeof(wh));
-            if ((rc = eval(e))) return rc;
+            ch.push_back(e);
+            if ((rc = eval_chain(ch))) return rc;
             k_controller<<<(nf + 127) / 128, 128, 0, stream>>>(d_films, nf, 3, req);
             CUDA_TRY(cudaGetLastError());
             launches += 1;
@@ -1432,7 +1473,11 @@ struct Engine final : EngineBase {
 
     // Per-pass CUDA-event timing of one representative RK45 stage evaluation
     // (stage 4: three-term combination) repeated `reps` times on the stream.
-    int profile_stage(const llg_params* p, int fmask, int reps, double* ms3) override {
+    // Device time per pass of one RK45 stage (stage 4 of the tableau, CUDA events on
+    // the solver stream): ms[0] row forward, ms[1] column, ms[2] row inverse (the
+    // transform and the streaming torque kernel), ms[3] the fused row pass that ends
+    // this stage and starts the next (0 where no segment fuses).
+    int profile_stage(const llg_params* p, int fmask, int reps, double* ms4) override {
         int rc;
         if ((rc = apply_params(p))) return rc;
         if ((rc = set_control(idle_control(), nullptr, nullptr, true))) return rc;
@@ -1440,9 +1485,13 @@ struct Engine final : EngineBase {
         e.rhs = RHS_LLG;
         combo(e, MB_S0, {KB_K1, KB_K2, KB_K3}, {dp5::A41, dp5::A42, dp5::A43});
         e.k_out = KB_K4;
-        cudaEvent_t ev[4];
+        EvalSpec f = e;
+        combo(f, MB_S1, {KB_K1, KB_K2, KB_K3, KB_K4}, {dp5::A51, dp5::A52, dp5::A53, dp5::A54});
+        f.k_out = KB_K5;
+        cudaEvent_t ev[5];
         for (auto& x : ev) CUDA_TRY(cudaEventCreate(&x));
-        double acc[3] = {0, 0, 0};
+        double acc[4] = {0, 0, 0, 0};
+        bool any_fused = false;
         for (int r = 0; r < reps; ++r) {
             CUDA_TRY(cudaEventRecord(ev[0], stream));
             for (auto& sg : rseg) CUDA_TRY(launch_one<R>(0, e, sg, stream));
@@ -1452,15 +1501,22 @@ struct Engine final : EngineBase {
             CUDA_TRY(cudaEventRecord(ev[2], stream));
             for (auto& sg : rseg) CUDA_TRY(launch_one<R>(2, e, sg, stream));
             CUDA_TRY(cudaEventRecord(ev[3], stream));
-            CUDA_TRY(cudaEventSynchronize(ev[3]));
-            for (int q = 0; q < 3; ++q) {
+            for (auto& sg : rseg)
+                if (can_fuse(e, f, sg)) {
+                    CUDA_TRY(launch_fused<R>(e, f, sg, stream));
+                    any_fused = true;
+                }
+            CUDA_TRY(cudaEventRecord(ev[4], stream));
+            CUDA_TRY(cudaEventSynchronize(ev[4]));
+            for (int q = 0; q < 4; ++q) {
                 float ms = 0.f;
                 CUDA_TRY(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
                 acc[q] += ms;
             }
         }
         for (auto& x : ev) cudaEventDestroy(x);
-        for (int q = 0; q < 3; ++q) ms3[q] = acc[q] / reps;
+        for (int q = 0; q < 4; ++q) ms4[q] = acc[q] / reps;
+        if (!any_fused) ms4[3] = 0.0;
         return LLG_OK;
     }
 
@@ -1720,10 +1776,10 @@ int llg_demag_kernel_kspace(llg_solver* s, double* out) {
     if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");
     return rc ? rc : s->eng->kernel_kspace(0, out);
 }
-int llg_profile_stage(llg_solver* s, const llg_params* p, int32_t fmask, int32_t reps, double* ms3) {
+int llg_profile_stage(llg_solver* s, const llg_params* p, int32_t fmask, int32_t reps, double* ms4) {
     int rc = bind(s);
-    if (!rc && (!p || !ms3 || reps < 1)) rc = set_error(LLG_ERR_INVALID, "bad argument");
-    return rc ? rc : s->eng->profile_stage(p, fmask, reps, ms3);
+    if (!rc && (!p || !ms4 || reps < 1)) rc = set_error(LLG_ERR_INVALID, "bad argument");
+    return rc ? rc : s->eng->profile_stage(p, fmask, reps, ms4);
 }
 int llg_solver_launch_count(llg_solver* s, int64_t* out) {
     int rc = bind(s);

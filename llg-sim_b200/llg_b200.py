@@ -438,9 +438,10 @@ class Solver:
         return out.value
 
     def profile_stage(self, params, field_mask=FULL, reps=20):
-        """Milliseconds per pass (row forward, column, row inverse) of one RK45 stage."""
+        """Milliseconds per pass of one RK45 stage: row forward, column, row inverse,
+        fused row pass (ending the stage and starting the next; 0 if unused)."""
         p = params._c()
-        out = np.empty(3)
+        out = np.empty(4)
         _check(lib().llg_profile_stage(self.h, C.byref(p), int(field_mask), int(reps), _dp(out)))
         return out
 

@@ -16,7 +16,7 @@ def test_library_exports_every_declared_symbol(gpu):
 
 
 def test_abi_version(gpu):
-    assert gpu.lib().llg_abi_version() == 1
+    assert gpu.lib().llg_abi_version() == 2
 
 
 def test_errors_are_statuses_not_aborts(gpu):
