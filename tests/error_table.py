@@ -95,10 +95,14 @@ def run_config(L, O, name, film, m0, kind, ctl, k_acc, precisions=(0, 1), fmask=
         gsv.set_state(m0)
         b = gsv.compute_demag_field()
         m_ref, m_gpu = replay(L, O, osv, gsv, m0, GAMMA, film.alpha, film.b_ext, kind, fmask, dts)
-        e_ref = osv.energy(m_ref, film.b_ext).total()
-        e_gpu = gsv.compute_energy(film.b_ext).total()
+        er = osv.energy(m_ref, film.b_ext)
+        eg = gsv.compute_energy(film.b_ext)
+        e_ref, e_gpu = er.total(), eg.total()
+        terms = {t: {"ref_J": getattr(er, t), "abs_err_J": abs(getattr(eg, t) - getattr(er, t))}
+                 for t in ("exchange", "anisotropy", "zeeman", "dmi", "demag")}
         out["fp64" if prec else "fp32"] = {"h_demag": field_err(b, b_ref), "m": state_err(m_gpu, m_ref),
-                                           "energy_rel": abs(e_gpu - e_ref) / max(abs(e_ref), 1e-300)}
+                                           "energy_rel": abs(e_gpu - e_ref) / max(abs(e_ref), 1e-300),
+                                           "energy_J": e_ref, "energy_terms": terms}
         gsv.close()
     osv.close()
     return out
