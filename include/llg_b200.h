@@ -398,6 +398,33 @@ int llg_warmstart_forward(llg_warmstart* w, int64_t nimg, int64_t ny, int64_t nx
                           const uint8_t* mask, const double* b_ext, double* out_aos);
 /* replace every film's state by the proposal computed from it on the device; b_ext [n][3] */
 int llg_batch_warm_start(llg_batch* b, llg_warmstart* w, const double* b_ext);
+/* Bound (in polls) of the network's tensor-core waits; a wait that runs out makes
+ * the call return LLG_ERR_TIMEOUT and the next call starts clean. */
+int llg_warmstart_set_spin_limit(llg_warmstart* w, int64_t polls);
+
+/* Training of the network on the GPU with the same tensor-core convolutions
+ * (forward, input gradient) plus a tensor-core weight-gradient kernel; FP32
+ * master weights and Adam on the device.  A minibatch is nimg films of ny x nx
+ * cells given by DEVICE pointers: m0 and target FP32 SoA planes with image
+ * stride 3*ny*nx (the initial and the relaxed states), mask uint8 [nimg][ny*nx]
+ * or NULL, bext double [nimg][3].  The loss is the mean over film cells of
+ * 1 - cos(angle) between the normalised output and the target.
+ *   llg_wstrain_gradients: loss and the gradient of the mean loss (host FP32,
+ *     the parameter layout; grad may be NULL), parameters unchanged;
+ *   llg_wstrain_step: one Adam step (lr, beta1, beta2, eps); loss may be NULL,
+ *     then the call does not synchronise;
+ *   llg_wstrain_get_params: the current FP32 parameters (host). */
+typedef struct llg_wstrain llg_wstrain;
+int llg_wstrain_create(llg_ctx* ctx, const float* params, int64_t n_params, int64_t max_cells, llg_wstrain** out);
+int llg_wstrain_destroy(llg_wstrain* t);
+int llg_wstrain_set_spin_limit(llg_wstrain* t, int64_t polls);
+int llg_wstrain_gradients(llg_wstrain* t, int64_t nimg, int64_t ny, int64_t nx, const float* m0, const uint8_t* mask,
+                          const double* bext, const float* target, double* loss, float* grad);
+int llg_wstrain_step(llg_wstrain* t, int64_t nimg, int64_t ny, int64_t nx, const float* m0, const uint8_t* mask,
+                     const double* bext, const float* target, float lr, float beta1, float beta2, float eps,
+                     double* loss);
+int llg_wstrain_sync(llg_wstrain* t);
+int llg_wstrain_get_params(llg_wstrain* t, float* out);
 
 #ifdef __cplusplus
 }

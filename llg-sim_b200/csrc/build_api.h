@@ -98,7 +98,8 @@ struct Net;
 long long net_param_count();
 cudaError_t net_create(const float* params, long long n, int device, Net** out);
 void net_destroy(Net* net);
-int net_error();
+int net_error(Net* net);
+void net_set_spin_limit(Net* net, long long polls);
 template <typename R>
 cudaError_t net_apply(Net* net, const R* m_in, R* m_out, const uint8_t* mask, const double* bext_host, int nimg,
                       int ny, int nx, cudaStream_t s);

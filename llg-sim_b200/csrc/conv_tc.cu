@@ -1,250 +1,16 @@
-// conv_tc.cu — the learned warm-start network on the 5th-generation tensor cores.
-//
-// Network (no reference counterpart): six 3x3 convolutions with zero padding,
-// 32 channels, ReLU between layers.  Input per cell: (mx, my, mz, inside, bx, by,
-// bz) with b = B_ext / 0.05 T, channel-padded to 16; output: three channels,
-// normalised to a unit vector inside the film and zero in holes.  Weights and
-// activations are BF16, accumulation FP32, bias FP32.
-//
-// One CTA computes a tile of 128 cells x N output channels as an implicit GEMM
-// D[128 x N] = A[128 x K] * B[N x K]^T with K = 9 * Cin:
-//   * the im2col rows of the tile (A) and the layer's weights (B) are written to
-//     shared memory in the no-swizzle K-major core-matrix layout (8 rows x 16 B
-//     per core matrix; core matrices along K 128 B apart, along M/N K*16 B apart);
-//   * one thread issues K/16 tcgen05.mma (kind::f16, BF16 x BF16 -> FP32) into a
-//     32-column TMEM accumulator and commits them to an mbarrier;
-//   * each warp reads its 32 TMEM lanes with tcgen05.ld and applies bias,
-//     activation and the store (or the final normalisation).
-// Waits are bounded; a wait that runs out records an error and the CTA frees its
-// TMEM before returning.
+// conv_tc.cu — host side of the learned warm-start network's inference: weights
+// packed for the tensor-core convolution (conv_tc.cuh), activation scratch, and
+// the proposal of a film batch's states.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
-#include "async_copy.cuh"
-
-namespace llg {
-namespace ws {
-
-constexpr int kTile = 128;       // cells per CTA (MMA M)
-constexpr int kCh = 32;          // hidden channels
-constexpr int kCin0 = 16;        // padded input channels (7 used)
-constexpr int kNout = 16;        // padded output channels of the last layer (3 used)
-constexpr int kLayers = 6;
-constexpr float kFieldScale = 1.0f / 0.05f;
-
-__device__ int g_ws_error;       // set when an mbarrier wait ran out
-
-struct Layer {
-    const __nv_bfloat16* w;      // [npad][9*cin] row-major, k = tap*cin + ci, tap = ky*3 + kx
-    const float* b;              // [npad]
-    int cin, npad, nreal, relu;
-};
-
-__host__ __device__ constexpr size_t conv_smem_bytes(int cin, int npad) {
-    return (size_t)kTile * 9 * cin * 2 + (size_t)npad * 9 * cin * 2;
-}
-
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
-           (1ull << 46);   // descriptor version for tcgen05; no swizzle, base offset 0
-}
-
-__device__ __forceinline__ uint32_t instr_desc_bf16(int n) {
-    // D f32, A bf16, B bf16, both K-major, N >> 3 at bit 17, M >> 4 at bit 24
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTile >> 4) << 24);
-}
-
-template <int NCOL>
-__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[NCOL]);
-
-template <>
-__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-template <>
-__device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float (&v)[32]) {
-    float* lo = v;
-    float* hi = v + 16;
-    float (&a)[16] = *reinterpret_cast<float(*)[16]>(lo);
-    float (&b)[16] = *reinterpret_cast<float(*)[16]>(hi);
-    tmem_ld<16>(taddr, a);
-    tmem_ld<16>(taddr + 16, b);
-}
-
-// One 3x3 convolution layer over nimg images of H x W cells (NHWC, C = cin).
-// Hidden layers write BF16 NHWC with C = 32; the last layer (NOUT = 16) writes
-// the normalised unit vector to m_out (SoA planes of `R`, one film per image,
-// cell stride H*W) with zero where mask == 0.
-template <int NCOL, typename R>
-__global__ void __launch_bounds__(kTile) k_conv3x3_tc(const __nv_bfloat16* __restrict__ x, int nimg, int H, int W,
-                                                      Layer L, __nv_bfloat16* __restrict__ y, R* __restrict__ m_out,
-                                                      const uint8_t* __restrict__ mask) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bar;
-    __shared__ uint32_t tmem_base;
-    const int cin = L.cin, K = 9 * cin;
-    const uint32_t sbo = (uint32_t)K * 16;   // bytes between 8-row groups
-    unsigned char* As = smem;
-    unsigned char* Bs = smem + (size_t)kTile * K * 2;
-    const int t = threadIdx.x, warp = t >> 5;
-    const long long hw = (long long)H * W;
-    const long long p = (long long)blockIdx.x * kTile + t;
-    const bool valid = p < (long long)nimg * hw;
-
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_addr(&tmem_base)),
-                     "r"(NCOL < 32 ? 32 : NCOL)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    if (t == 0) {
-        mbar_init(&bar, 1);
-        mbar_init_fence();
-    }
-    // im2col row of cell p: 9 taps x cin channels, 16-byte chunks of 8 channels
-    {
-        const int img = valid ? (int)(p / hw) : 0;
-        const int rem = valid ? (int)(p - (long long)img * hw) : 0;
-        const int yy = rem / W, xx = rem - (rem / W) * W;
-        const int groups = cin / 8;
-        unsigned char* arow = As + (size_t)(t >> 3) * sbo + (size_t)(t & 7) * 16;
-        for (int tap = 0; tap < 9; ++tap) {
-            const int sy = yy + tap / 3 - 1, sx = xx + tap % 3 - 1;
-            const bool in = valid && sy >= 0 && sy < H && sx >= 0 && sx < W;
-            const uint4* src = reinterpret_cast<const uint4*>(x + (((long long)img * H + (in ? sy : 0)) * W +
-                                                                     (in ? sx : 0)) * cin);
-            for (int g = 0; g < groups; ++g) {
-                const uint4 v = in ? src[g] : make_uint4(0u, 0u, 0u, 0u);
-                const int k0 = tap * cin + g * 8;
-                *reinterpret_cast<uint4*>(arow + (size_t)(k0 >> 3) * 128) = v;
-            }
-        }
-    }
-    // weights: npad rows of K
-    {
-        const int chunks = L.npad * (K / 8);
-        for (int c = t; c < chunks; c += kTile) {
-            const int n = c / (K / 8), kc = c - n * (K / 8);
-            const uint4 v = reinterpret_cast<const uint4*>(L.w + (size_t)n * K)[kc];
-            *reinterpret_cast<uint4*>(Bs + (size_t)(n >> 3) * sbo + (size_t)kc * 128 + (size_t)(n & 7) * 16) = v;
-        }
-    }
-    fence_async_smem();   // generic-proxy tile writes -> tensor-core reads
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = tmem_base;
-    if (t == 0) {
-        const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs);
-        const uint32_t idesc = instr_desc_bf16(L.npad);
-        for (int kk = 0; kk < K / 16; ++kk) {
-            const uint64_t da = smem_desc(a0 + kk * 256, 128, sbo);
-            const uint64_t db = smem_desc(b0 + kk * 256, 128, sbo);
-            const uint32_t acc = kk > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                "l"(da), "l"(db), "r"(idesc), "r"(acc)
-                : "memory");
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_addr(&bar))
-                     : "memory");
-    }
-    const bool done = mbar_wait(&bar, 0);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!done) {
-        if (t == 0) atomicExch(&g_ws_error, 1);
-        mbar_wait(&bar, 0);   // give the MMAs one more bounded wait before the TMEM is freed
-    } else {
-        float acc[NCOL];
-        tmem_ld<NCOL>(tmem + ((uint32_t)(warp * 32) << 16), acc);
-        if (valid) {
-            if (m_out == nullptr) {
-                alignas(16) __nv_bfloat16 o[NCOL];
-#pragma unroll
-                for (int c = 0; c < NCOL; ++c) {
-                    float v = acc[c] + L.b[c];
-                    if (L.relu) v = fmaxf(v, 0.0f);
-                    o[c] = __float2bfloat16(v);
-                }
-                uint4* dst = reinterpret_cast<uint4*>(y + p * NCOL);
-#pragma unroll
-                for (int q = 0; q < NCOL / 8; ++q) dst[q] = reinterpret_cast<const uint4*>(o)[q];
-            } else {
-                const int img = (int)(p / hw);
-                const long long cell = p - (long long)img * hw;
-                float v0 = acc[0] + L.b[0], v1 = acc[1] + L.b[1], v2 = acc[2] + L.b[2];
-                const bool inside = mask == nullptr || mask[p] != 0;
-                const float nn = v0 * v0 + v1 * v1 + v2 * v2;
-                if (!inside) {
-                    v0 = v1 = v2 = 0.0f;
-                } else if (nn > 0.0f) {
-                    const float inv = 1.0f / sqrtf(nn);
-                    v0 *= inv; v1 *= inv; v2 *= inv;
-                } else {
-                    v0 = 0.0f; v1 = 0.0f; v2 = 1.0f;   // normalize(0) = +z (vec3.rs:21-25)
-                }
-                R* mo = m_out + (size_t)img * 3 * hw;
-                mo[cell] = (R)v0;
-                mo[hw + cell] = (R)v1;
-                mo[2 * hw + cell] = (R)v2;
-            }
-        }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(NCOL < 32 ? 32 : NCOL)
-                     : "memory");
-}
-
-// Network input of image f from SoA planes m (R), mask and the image's field.
-template <typename R>
-__global__ void k_ws_input(const R* __restrict__ m, const uint8_t* __restrict__ mask, const double* __restrict__ bext,
-                           int nimg, long long hw, __nv_bfloat16* __restrict__ x) {
-    const long long total = (long long)nimg * hw;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total;
-         p += (long long)gridDim.x * blockDim.x) {
-        const int img = (int)(p / hw);
-        const long long cell = p - (long long)img * hw;
-        const R* mi = m + (size_t)img * 3 * hw;
-        const bool inside = mask == nullptr || mask[p] != 0;
-        alignas(16) __nv_bfloat16 v[kCin0];
-        const float in = inside ? 1.0f : 0.0f;
-        v[0] = __float2bfloat16(in * (float)mi[cell]);
-        v[1] = __float2bfloat16(in * (float)mi[hw + cell]);
-        v[2] = __float2bfloat16(in * (float)mi[2 * hw + cell]);
-        v[3] = __float2bfloat16(in);
-        v[4] = __float2bfloat16((float)bext[3 * img + 0] * kFieldScale);
-        v[5] = __float2bfloat16((float)bext[3 * img + 1] * kFieldScale);
-        v[6] = __float2bfloat16((float)bext[3 * img + 2] * kFieldScale);
-#pragma unroll
-        for (int c = 7; c < kCin0; ++c) v[c] = __float2bfloat16(0.0f);
-        uint4* dst = reinterpret_cast<uint4*>(x + p * kCin0);
-        dst[0] = reinterpret_cast<const uint4*>(v)[0];
-        dst[1] = reinterpret_cast<const uint4*>(v)[1];
-    }
-}
-
-}  // namespace ws
-}  // namespace llg
+#include "conv_tc.cuh"
 
 // ---------------------------------------------------------------------------
 // Host side
@@ -256,6 +22,8 @@ namespace ws {
 
 struct Net {
     int device = 0;
+    int* err = nullptr;            // device flag: a tensor-core wait ran out during the last apply
+    long long spin = kMbarSpinLimit;
     __nv_bfloat16* w[kLayers] = {};
     float* b[kLayers] = {};
     Layer L[kLayers];
@@ -288,6 +56,7 @@ void net_destroy(Net* net) {
     cudaFree(net->h[0]);
     cudaFree(net->h[1]);
     cudaFree(net->bext);
+    cudaFree(net->err);
     cudaSetDevice(prev);
     delete net;
 }
@@ -317,15 +86,21 @@ cudaError_t net_create(const float* params, long long n, int device, Net** out) 
         if (e == cudaSuccess) e = cudaMemcpy(net->b[l], b.data(), b.size() * sizeof(float), cudaMemcpyHostToDevice);
         net->L[l] = Layer{net->w[l], net->b[l], cin, npad, co_r, l < kLayers - 1 ? 1 : 0};
     }
+    if (e == cudaSuccess) e = cudaMalloc(&net->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(net->err, 0, sizeof(int));
     if (e == cudaSuccess) {
-        const size_t smax = conv_smem_bytes(kCh, kCh);
-        e = cudaFuncSetAttribute(k_conv3x3_tc<kCh, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+        const int smax = (int)conv_smem_bytes(kCh, kCh);
+        e = cudaFuncSetAttribute(k_conv3x3_tc<kCh, EPI_HIDDEN, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smax);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_conv3x3_tc<kNout, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+            e = cudaFuncSetAttribute(k_conv3x3_tc<kNout, EPI_FINAL_NORM, float>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_conv3x3_tc<kCh, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+            e = cudaFuncSetAttribute(k_conv3x3_tc<kCh, EPI_HIDDEN, double>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_conv3x3_tc<kNout, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+            e = cudaFuncSetAttribute(k_conv3x3_tc<kNout, EPI_FINAL_NORM, double>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
     }
     if (e != cudaSuccess) {
         net_destroy(net);
@@ -359,11 +134,15 @@ static cudaError_t ensure_scratch(Net* net, long long cells, int nimg) {
     return cudaSuccess;
 }
 
-int net_error() {
+// Whether a tensor-core wait of the last apply ran out (reads the flag that
+// net_apply cleared at its start; call after the apply's stream is synchronised).
+int net_error(Net* net) {
     int v = 0;
-    cudaMemcpyFromSymbol(&v, g_ws_error, sizeof(int));
+    if (cudaMemcpy(&v, net->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
     return v;
 }
+
+void net_set_spin_limit(Net* net, long long polls) { net->spin = polls; }
 
 // Proposal for nimg images of ny x nx cells (SoA planes of R, image stride 3*ny*nx):
 // m_out may alias m_in (the input is consumed by the first layer).
@@ -373,6 +152,8 @@ cudaError_t net_apply(Net* net, const R* m_in, R* m_out, const uint8_t* mask, co
     const long long hw = (long long)ny * nx, cells = hw * nimg;
     if (cells <= 0) return cudaSuccess;
     cudaError_t e = ensure_scratch(net, cells, nimg);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(net->err, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
     e = cudaMemcpyAsync(net->bext, bext_host, (size_t)nimg * 3 * sizeof(double), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return e;
@@ -385,10 +166,13 @@ cudaError_t net_apply(Net* net, const R* m_in, R* m_out, const uint8_t* mask, co
         const size_t smem = conv_smem_bytes(L.cin, L.npad);
         if (l < kLayers - 1) {
             __nv_bfloat16* nxt = net->h[l & 1];
-            k_conv3x3_tc<kCh, R><<<grid, kTile, smem, s>>>(cur, nimg, ny, nx, L, nxt, nullptr, nullptr);
+            k_conv3x3_tc<kCh, EPI_HIDDEN, R><<<grid, kTile, smem, s>>>(cur, nimg, ny, nx, L, nxt, nullptr, nullptr,
+                                                                        nullptr, nullptr, net->err, net->spin);
             cur = nxt;
         } else {
-            k_conv3x3_tc<kNout, R><<<grid, kTile, smem, s>>>(cur, nimg, ny, nx, L, nullptr, m_out, mask);
+            k_conv3x3_tc<kNout, EPI_FINAL_NORM, R><<<grid, kTile, smem, s>>>(cur, nimg, ny, nx, L, nullptr, m_out,
+                                                                              nullptr, mask, nullptr, net->err,
+                                                                              net->spin);
         }
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;

@@ -64,7 +64,10 @@ FastCfg fast_config(int nx, int ny) {
         c.smem_col = ColCfg<R, L>::SMEM;
         c.twp_col_size = TwTab<R, L>::size;
     });
-    c.ok_row = okr && c.smem_row <= kSmemMax;
+    // The register-FFT row kernels move the spectrum of consecutive rows as 16-byte
+    // pieces of the column-major X[c][kx][j]: in FP32 a piece is two rows, so the
+    // column stride ny must be even for every piece to start on a 16-byte boundary.
+    c.ok_row = okr && c.smem_row <= kSmemMax && (sizeof(R) == 8 || ny % 2 == 0);
     c.ok_col = okc && c.smem_col + kStaticSmemCol <= kSmemMax;
     c.ok = c.ok_row && c.ok_col;
     return c;

@@ -817,7 +817,7 @@ struct Engine final : EngineBase {
         for (int e = 0; e < nf; ++e) iv[e] = true;
         if ((rc = set_control(idle_control(), nullptr, iv.get(), true))) return rc;
         CUDA_TRY(cudaStreamSynchronize(stream));
-        if (ws::net_error()) return set_error(LLG_ERR_TIMEOUT, "warm-start network: tensor-core wait timed out");
+        if (ws::net_error(net)) return set_error(LLG_ERR_TIMEOUT, "warm-start network: tensor-core wait timed out");
         return LLG_OK;
     }
 
@@ -1892,6 +1892,13 @@ int llg_warmstart_create(llg_ctx* ctx, const float* params, int64_t n_params, ll
     return LLG_OK;
 }
 
+int llg_warmstart_set_spin_limit(llg_warmstart* w, int64_t polls) {
+    if (!w) return set_error(LLG_ERR_INVALID, "null argument");
+    if (polls < 0) return set_error(LLG_ERR_INVALID, "negative spin limit");
+    llg::ws::net_set_spin_limit(w->net, polls);
+    return LLG_OK;
+}
+
 int llg_warmstart_destroy(llg_warmstart* w) {
     if (!w) return LLG_OK;
     cudaSetDevice(w->device);
@@ -1925,7 +1932,7 @@ int llg_warmstart_forward(llg_warmstart* w, int64_t nimg, int64_t ny, int64_t nx
     cudaFree(d_m);
     cudaFree(d_mask);
     if (e != cudaSuccess) return set_error(LLG_ERR_CUDA, "warm-start forward: %s", cudaGetErrorString(e));
-    if (llg::ws::net_error()) return set_error(LLG_ERR_TIMEOUT, "warm-start network: tensor-core wait timed out");
+    if (llg::ws::net_error(w->net)) return set_error(LLG_ERR_TIMEOUT, "warm-start network: tensor-core wait timed out");
     for (long long im = 0; im < nimg; ++im)
         for (long long c = 0; c < hw; ++c)
             for (int q = 0; q < 3; ++q) out_aos[3 * (im * hw + c) + q] = soa[(size_t)im * 3 * hw + q * hw + c];

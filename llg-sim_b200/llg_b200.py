@@ -228,6 +228,15 @@ def lib():
             "llg_warmstart_destroy": (C.c_int, [vp]),
             "llg_warmstart_forward": (C.c_int, [vp, i64, i64, i64, dp, vp, dp, dp]),
             "llg_batch_warm_start": (C.c_int, [vp, vp, dp]),
+            "llg_warmstart_set_spin_limit": (C.c_int, [vp, i64]),
+            "llg_wstrain_create": (C.c_int, [vp, P(C.c_float), i64, i64, P(vp)]),
+            "llg_wstrain_destroy": (C.c_int, [vp]),
+            "llg_wstrain_set_spin_limit": (C.c_int, [vp, i64]),
+            "llg_wstrain_gradients": (C.c_int, [vp, i64, i64, i64, vp, vp, vp, vp, dp, P(C.c_float)]),
+            "llg_wstrain_step": (C.c_int, [vp, i64, i64, i64, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float,
+                                           C.c_float, dp]),
+            "llg_wstrain_sync": (C.c_int, [vp]),
+            "llg_wstrain_get_params": (C.c_int, [vp, P(C.c_float)]),
             "llg_init_random": (None, [i64, C.c_uint64, dp]),
             "llg_init_uniform_with_noise": (None, [i64, dp, C.c_double, C.c_uint64, dp]),
         }
@@ -864,6 +873,10 @@ class WarmStartNet:
         except Exception:
             pass
 
+    def set_spin_limit(self, polls):
+        """Bound (in polls) of the network's tensor-core waits."""
+        _check(lib().llg_warmstart_set_spin_limit(self.h, int(polls)))
+
     def forward(self, m, mask, b_ext, ny, nx):
         """m [nimg, ny*nx, 3] (or one image), mask [nimg, ny*nx] or None, b_ext [nimg, 3]."""
         m = np.ascontiguousarray(np.asarray(m, dtype=np.float64))
@@ -875,6 +888,61 @@ class WarmStartNet:
             mk = np.ascontiguousarray(np.asarray(mask).reshape(-1).astype(np.uint8))
             mp = mk.ctypes.data_as(C.c_void_p)
         _check(lib().llg_warmstart_forward(self.h, nimg, int(ny), int(nx), _dp(m), mp, _dp(be), _dp(out)))
+        return out
+
+
+class WarmStartTrainer:
+    """Training of the warm-start network on the GPU by this library's tensor-core
+    kernels (forward, input gradient, weight gradient) with Adam on FP32 master
+    weights.  Minibatches are device pointers (integers, e.g. torch tensors'
+    data_ptr()): m0 and target FP32 SoA planes [nimg][3][ny][nx], mask uint8
+    [nimg][ny][nx] or 0, bext float64 [nimg][3]."""
+
+    def __init__(self, params, max_cells, device=0):
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float32).reshape(-1))
+        h = C.c_void_p()
+        _check(lib().llg_wstrain_create(_ctx(device), p.ctypes.data_as(C.POINTER(C.c_float)), p.size,
+                                        int(max_cells), C.byref(h)))
+        self.h = h
+        self.n = p.size
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().llg_wstrain_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_spin_limit(self, polls):
+        _check(lib().llg_wstrain_set_spin_limit(self.h, int(polls)))
+
+    def gradients(self, nimg, ny, nx, m0_ptr, mask_ptr, bext_ptr, target_ptr):
+        """(mean loss, gradient of the mean loss in the parameter layout); parameters unchanged."""
+        loss = C.c_double()
+        g = np.empty(self.n, dtype=np.float32)
+        _check(lib().llg_wstrain_gradients(self.h, int(nimg), int(ny), int(nx), m0_ptr, mask_ptr or None, bext_ptr,
+                                           target_ptr, C.byref(loss), g.ctypes.data_as(C.POINTER(C.c_float))))
+        return loss.value, g
+
+    def step(self, nimg, ny, nx, m0_ptr, mask_ptr, bext_ptr, target_ptr, lr, beta1=0.9, beta2=0.999, eps=1e-8,
+             read_loss=True):
+        """One Adam step; returns the minibatch's mean loss (None with read_loss=False: no synchronisation)."""
+        loss = C.c_double()
+        _check(lib().llg_wstrain_step(self.h, int(nimg), int(ny), int(nx), m0_ptr, mask_ptr or None, bext_ptr,
+                                      target_ptr, float(lr), float(beta1), float(beta2), float(eps),
+                                      C.byref(loss) if read_loss else None))
+        return loss.value if read_loss else None
+
+    def sync(self):
+        _check(lib().llg_wstrain_sync(self.h))
+
+    def params(self):
+        out = np.empty(self.n, dtype=np.float32)
+        _check(lib().llg_wstrain_get_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
 
 

@@ -5,7 +5,7 @@ LLG_B200_COL_STAGED=1 select the unfused / staged kernels at solver creation."""
 import numpy as np
 import pytest
 
-from helpers import GAMMA, case, gpu_solver, holes_mask, random_m
+from helpers import GAMMA, case, gpu_solver, holes_mask, oracle_solver, random_m, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -13,7 +13,7 @@ CASES = [
     # nx, ny, dmi, ku, masked
     (1024, 64, 3e-3, 8e5, False),
     (256, 96, 1e-3, 0.0, True),
-    (128, 33, None, 5e4, False),
+    (128, 34, None, 5e4, False),   # partial last row block
     (64, 64, -2e-3, 1e5, True),
 ]
 
@@ -75,6 +75,29 @@ def test_direct_column_equals_staged(orc, gpu, monkeypatch):
     direct.set_state(m)
     staged.set_state(m)
     assert np.array_equal(direct.compute_demag_field(), staged.compute_demag_field())
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_odd_rows_with_power_of_two_width(orc, gpu, prec):
+    """nx = 128 with an odd ny: FP32 takes the generic row kernels (the register-FFT
+    row kernels need 16-byte aligned two-row pieces of the spectrum), FP64 the fast
+    ones; both match the oracle."""
+    nx, ny = 128, 33
+    c = case(nx, ny, dmi=1e-3, k_u=5e4)
+    o = oracle_solver(orc, c)
+    g = gpu_solver(gpu, c, prec)
+    m = random_m(orc, nx * ny, 9)
+    g.set_state(m)
+    p = gpu.LLGParams(GAMMA, 0.1, 1e-13, (0.01, 0.0, 0.0))
+    assert rel_err(g.build_h_eff(p, 2), o.build_h_eff(m, (0.01, 0.0, 0.0), 2)) <= (1e-9 if prec else 2e-5)
+    po = orc.make_params(GAMMA, 0.1, 1e-13, (0.01, 0.0, 0.0))
+    mo = m.copy()
+    for _ in range(4):
+        ro = o.step_rk45(mo, po, 2, 1e-5, 0.8, 1e-19, 1e-11)
+        rg = g.step_rk45(p, 2, 1e-5, 0.8, 1e-19, 1e-11)
+        assert ro[1] == rg[1]
+        p.dt = po.dt
+    assert np.abs(g.get_state() - mo).max() <= (1e-12 if prec else 1e-6)
 
 
 def test_profile_reports_fused_pass(gpu):
