@@ -326,63 +326,92 @@ def flow_leg(L, torch, stream):
     return out
 
 
-def warmstart_leg(L, torch, stream, max_over_ranks, n_films=16, size=256):
-    """Holey films (0-6 holes, D U[0,2e-3], 0-30 mT), random m0, FP32 batched relax to
-    max |m x B| 1e-3 T: plain start vs the learned warm start (network on the tensor
-    cores, then relax).  Device-clock wall times of both arms; the final energies are
-    checked against the FP64 oracle evaluated on the GPU's final states."""
+def warmstart_leg(L, torch, stream, max_over_ranks, n_films=16, size=256, torque=1e-6, fp32_torque=1e-3,
+                  max_steps=60000, weights=None):
+    """c5: holey films (0-6 holes, D U[0,2e-3], 0-30 mT), random m0, relaxed to max
+    |m x B| <= `torque` (1e-6 T) in two stages: the batched FP32 device relax to
+    `fp32_torque` (near the FP32 field round-off floor), then the FP64 device relax from
+    the FP32 state to `torque`.  Arms: plain start, and the learned proposal (network on
+    the tensor cores) then the same two stages.  Device-clock wall time per arm (the
+    FP32 -> FP64 hand-over through host memory included).  Per film: the final FP64
+    energies of both arms; a learned film whose energy differs from the plain one by
+    more than 1e-6 relative falls back to the plain start, and the fallback's cost (the
+    plain pipeline re-run for those films) is added to the learned arm."""
     import workloads as W
 
-    wpath = os.path.join(ROOT, "llg-sim_b200", "weights", "warmstart_holey128.npy")
+    wpath = weights or os.path.join(ROOT, "llg-sim_b200", "weights", "warmstart_holey128.npy")
     net = L.WarmStartNet(np.load(wpath))
     films, rx = W.holey_film_batch(n_films, size, seed=77)
-    st = dict(torque_threshold=1e-3, max_err=rx["max_err"], headroom=rx["headroom"], dt_min=rx["dt_min"],
-              dt_max=rx["dt_max"], max_accepted_steps=60000)
-    out = {"workload": f"{n_films} films {size}x{size}, 4x4x3 nm, 0-6 holes r 8-24 cells, D U[0,2e-3], 0-30 mT "
-                       f"in-plane, random m0, FP32 relax to max|m x B| 1e-3 T (RK23, max 60000 steps)",
-           "weights": "llg-sim_b200/weights/warmstart_holey128.npy (trained on 1024 relaxed 128x128 films)"}
-    finals = {}
-    for arm in ("plain", "learned"):
-        b = L.Batch([f.grid(L) for f in films], [f.material(L) for f in films], L.FP32, masks=[f.mask for f in films])
-        b.set_stream(stream.cuda_stream)
-        for i, f in enumerate(films):
-            m = L.init_random(f.n, 900000 + i)
-            m[f.mask == 0] = 0.0
-            b.set_state(i, m)
-        P = [L.LLGParams(GAMMA, f.alpha, rx["dt0"], f.b_ext) for f in films]
+    m0 = []
+    for i, f in enumerate(films):
+        m = L.init_random(f.n, 900000 + i)
+        m[f.mask == 0] = 0.0
+        m0.append(m)
+    s32 = dict(torque_threshold=fp32_torque, max_err=rx["max_err"], headroom=rx["headroom"], dt_min=rx["dt_min"],
+               dt_max=rx["dt_max"], max_accepted_steps=max_steps)
+    s64 = dict(s32, torque_threshold=torque)
+
+    def arm(idx, learned):
+        fs = [films[i] for i in idx]
+        grids = [f.grid(L) for f in fs]
+        mats = [f.material(L) for f in fs]
+        msk = [f.mask for f in fs]
+        bex = [f.b_ext for f in fs]
+        b32 = L.Batch(grids, mats, L.FP32, masks=msk)
+        b64 = L.Batch(grids, mats, L.FP64, masks=msk)
+        for b in (b32, b64):
+            b.set_stream(stream.cuda_stream)
+        for k, i in enumerate(idx):
+            b32.set_state(k, m0[i])
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        if arm == "learned":
-            b.warm_start(net, [f.b_ext for f in films])
-        reps = b.relax(P, L.FULL, L.RelaxSettings.default(**st))
+        if learned:
+            b32.warm_start(net, bex)
+        r32 = b32.relax([L.LLGParams(GAMMA, f.alpha, rx["dt0"], f.b_ext) for f in fs], L.FULL,
+                        L.RelaxSettings.default(**s32))
+        for k in range(len(fs)):
+            b64.set_state(k, b32.get_state(k))
+        r64 = b64.relax([L.LLGParams(GAMMA, f.alpha, rx["dt0"], f.b_ext) for f in fs], L.FULL,
+                        L.RelaxSettings.default(**s64))
         e1.record(stream)
         torch.cuda.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1))
-        en = [e.total() for e in b.compute_energy([f.b_ext for f in films])]
-        finals[arm] = ([b.get_state(i) for i in range(len(films))], en)
-        out[arm] = {"wall_s": ms * 1e-3, "steps_mean": float(np.mean([r.accepted_steps for r in reps])),
-                    "steps_max": int(max(r.accepted_steps for r in reps)),
-                    "converged": int(sum(r.stop_reason == 2 for r in reps)),
-                    "energy_mean_J": float(np.mean(en))}
-        b.close()
-    out["speedup"] = out["plain"]["wall_s"] / out["learned"]["wall_s"]
-    net.close()
-    try:
-        import oracle as O
+        en = np.array([e.total() for e in b64.compute_energy(bex)])
+        tq = np.array([r.final_torque_max if r.has_final_torque_max else np.inf for r in r64])
+        out = {"wall_s": ms * 1e-3, "fp32_steps_mean": float(np.mean([r.accepted_steps for r in r32])),
+               "fp64_steps_mean": float(np.mean([r.accepted_steps for r in r64])),
+               "fp64_steps_max": int(max(r.accepted_steps for r in r64)),
+               "at_cap": int(sum(r.accepted_steps >= max_steps for r in r64)),
+               "converged": int((tq <= torque).sum())}
+        b32.close()
+        b64.close()
+        return out, en, tq
 
-        worst = 0.0
-        for arm in ("plain", "learned"):
-            states, en = finals[arm]
-            for i, f in enumerate(films[:4]):
-                s = O.Solver(O.make_grid(f.nx, f.ny, f.dx, f.dy, f.dz),
-                             O.make_material(f.ms, f.a_ex, f.k_u, f.easy, f.dmi, f.demag), f.mask)
-                eo = s.energy(states[i], f.b_ext).total()
-                worst = max(worst, abs(en[i] - eo) / abs(eo))
-        out["energy_max_rel_diff_vs_fp64_oracle"] = worst
-    except Exception as exc:   # the oracle library is optional where the benchmark runs
-        out["energy_max_rel_diff_vs_fp64_oracle"] = f"unavailable: {exc}"
-    return out
+    all_idx = list(range(n_films))
+    plain, e_plain, t_plain = arm(all_idx, False)
+    learned, e_learn, t_learn = arm(all_idx, True)
+    rel = np.abs(e_learn - e_plain) / np.abs(e_plain)
+    differ = [i for i in all_idx if not rel[i] <= 1e-6]
+    fallback = {"films": len(differ), "wall_s": 0.0}
+    if differ:
+        fb, _, _ = arm(differ, False)
+        fallback["wall_s"] = fb["wall_s"]
+    net.close()
+    both = (t_plain <= torque) & (t_learn <= torque)
+    agree = rel[both] <= 1e-6
+    return {"workload": f"{n_films} films {size}x{size}, 4x4x3 nm, 0-6 holes r 8-24 cells, D U[0,2e-3], 0-30 mT "
+                        f"in-plane, alpha 0.5, random m0; relax to max|m x B| {torque:.0e} T: FP32 device relax to "
+                        f"{fp32_torque:.0e} T then FP64 device relax (RK23, at most {max_steps} steps per stage)",
+            "weights": os.path.relpath(wpath, ROOT), "plain": plain, "learned": learned,
+            "fallback": fallback, "learned_with_fallback_s": learned["wall_s"] + fallback["wall_s"],
+            "speedup": plain["wall_s"] / (learned["wall_s"] + fallback["wall_s"]),
+            "speedup_without_fallback": plain["wall_s"] / learned["wall_s"],
+            "films_converged_both": int(both.sum()),
+            "films_same_energy_1e-6": int(agree.sum()),
+            "energy_rel_diff": {"median": float(np.median(rel)), "max": float(rel.max()),
+                                "learned_lower": int(((e_learn < e_plain) & (rel > 1e-6)).sum()),
+                                "learned_higher": int(((e_learn > e_plain) & (rel > 1e-6)).sum())}}
 
 
 def amr_leg(L, reps=5):
@@ -637,6 +666,7 @@ def run_gpu(args):
     # row-inverse pass once (stage 7, with the error norm); the dominant kernel is
     # the one with the largest share of the step's device time.
     prof = s.profile_stage(p, fm, reps=30)
+    row_plan, col_plan = s.fft_plans()
     K1 = w["nx"] + 1
     x_bytes = 3 * K1 * w["ny"] * 8
     khat_bytes = K1 * (w["ny"] + 1) * 16
@@ -667,6 +697,7 @@ def run_gpu(args):
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "bytes_per_launch": bytes_pass[dom], "ms_per_launch": dom_ms,
                 "launches_per_step": {k: per_step[k] for k in live},
+                "fft_plans": {"row": row_plan, "column": col_plan},
                 "per_pass_ms": {k: _r(float(prof[names.index(k)])) for k in live},
                 "per_pass_frac": {k: _r(bytes_pass[k] / (float(prof[names.index(k)]) * 1e-3) / 1e9 / peak)
                                   for k in live}}
@@ -768,7 +799,7 @@ def run_gpu(args):
         flow = flow_leg(L, torch, stream)
     warm = None
     if not args.no_warmstart:
-        warm = warmstart_leg(L, torch, stream, max_over_ranks)
+        warm = warmstart_leg(L, torch, stream, max_over_ranks, n_films=args.warm_films, weights=args.warm_weights)
     amr = None
     if not args.no_amr and world == 1:
         amr = amr_leg(L)
@@ -822,6 +853,8 @@ def main():
     ap.add_argument("--no-amr", action="store_true")
     ap.add_argument("--no-sp4", action="store_true")
     ap.add_argument("--no-minimize", action="store_true")
+    ap.add_argument("--warm-films", type=int, default=16, help="films of the learned-warm-start leg (c5: 256)")
+    ap.add_argument("--warm-weights", default=None, help="network parameters (.npy) of the warm-start leg")
     ap.add_argument("--detail", default=None, help="also write every leg's full record to this JSON file")
     ap.add_argument("--cpu-leg", default=None, choices=sorted(CPU_VARIANTS), help=argparse.SUPPRESS)
     args = ap.parse_args()

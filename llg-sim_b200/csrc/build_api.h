@@ -50,28 +50,32 @@ struct LaunchGeom {
     int grid_fused;   // fused row pass (k_row_fused)
     bool any_demag;
     bool fuse_rows;   // end a stage and start the next in one row pass where possible
-    bool col_direct;  // column pass loads its spectrum straight into registers
+    int row_var;      // register-FFT radix plan of the row kernels (FPlan V)
+    int col_var;      // register-FFT radix plan of the column kernel (FPlan V)
     int fast_row;     // register-FFT row kernels for L = nx (0: generic kernels)
     int fast_col;     // register-FFT column kernel for L = ny (0: generic kernel)
     int row_threads;
     int col_threads;
 };
 
-// Register-FFT configuration for a film size: rows per block T, columns per
-// block, threads and shared memory; ok = false when the size has no fast path.
+// Register-FFT configuration for a film size per radix plan v (0 default, 1
+// alternative): rows per block T, columns per block NC, threads, shared memory,
+// pass-table sizes; ok_row / ok_col = false where the size has no such kernel.
 struct FastCfg {
-    bool ok;
-    bool ok_row, ok_col;   // a register-FFT row / column kernel exists for this nx / ny
-    int T, NC, row_threads, col_threads;
-    size_t smem_row, smem_col;
-    int twp_row_size, twp_col_size;
+    bool ok_row[2], ok_col[2];
+    int T[2], NC[2], row_threads[2], col_threads[2];
+    size_t smem_row[2], smem_col[2];
+    int twp_row_size[2], twp_col_size[2];
 };
 template <typename R>
 FastCfg fast_config(int nx, int ny);
-// Resident blocks per SM of the fast kernels (after prepare_eval_kernels).
+// Resident blocks per SM of the fast kernels of the given plans (after prepare_eval_kernels).
 template <typename R>
-void fast_occupancy(int nx, int ny, bool col_direct, int* fwd_blocks_per_sm, int* inv_blocks_per_sm,
+void fast_occupancy(int nx, int ny, int row_var, int col_var, int* fwd_blocks_per_sm, int* inv_blocks_per_sm,
                     int* full_blocks_per_sm, int* fused_blocks_per_sm, int* col_blocks_per_sm);
+// Pass twiddle tables of the register FFT of length L, plan v.
+template <typename R>
+cudaError_t build_pass_tables(void* out, int L, int v, cudaStream_t s);
 // Whether stage si's row inverse and stage sf's row forward can run as one fused
 // row pass on segment g (register-FFT rows, lean epilogue, sf's combination ends
 // with si's torque).
@@ -79,9 +83,6 @@ bool can_fuse(const EvalSpec& si, const EvalSpec& sf, const LaunchGeom& g);
 template <typename R>
 cudaError_t launch_fused(const EvalSpec& si, const EvalSpec& sf, const LaunchGeom& g, cudaStream_t s,
                          int* nk = nullptr);
-template <typename R>
-cudaError_t build_pass_tables(void* out_row, int nx, void* out_col, int ny, cudaStream_t s);
-
 template <typename R>
 cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t s);
 template <typename R>

@@ -28,6 +28,23 @@ bool dispatch_L(int L, F&& f) {
     }
 }
 
+// f(L, V) for a power-of-two length L and radix plan V that exist (FPlan::ok).
+template <typename R, typename F>
+bool dispatch_LV(int L, int V, F&& f) {
+    bool done = false;
+    dispatch_L<R>(L, [&](auto LC) {
+        constexpr int LL = decltype(LC)::value;
+        if (V == 0) {
+            f(LC, std::integral_constant<int, 0>{});
+            done = true;
+        } else if constexpr (FPlan<R, LL, 1>::ok) {
+            f(LC, std::integral_constant<int, 1>{});
+            done = true;
+        }
+    });
+    return done;
+}
+
 constexpr size_t kSmemMax = 227 * 1024;
 constexpr size_t kStaticSmemCol = 64;   // mbarriers and the timeout flag of k_column_fast
 
@@ -50,44 +67,37 @@ bool lean_err45_epilogue(const EvalSpec& e) {
 template <typename R>
 FastCfg fast_config(int nx, int ny) {
     FastCfg c{};
-    bool okr = dispatch_L<R>(nx, [&](auto LC) {
-        constexpr int L = decltype(LC)::value;
-        c.T = RowCfg<R, L>::T;
-        c.row_threads = RowCfg<R, L>::THREADS;
-        c.smem_row = RowCfg<R, L>::SMEM;
-        c.twp_row_size = TwTab<R, L>::size;
-    });
-    bool okc = dispatch_L<R>(ny, [&](auto LC) {
-        constexpr int L = decltype(LC)::value;
-        c.NC = ColCfg<R, L>::NC;
-        c.col_threads = ColCfg<R, L>::THREADS;
-        c.smem_col = ColCfg<R, L>::SMEM;
-        c.twp_col_size = TwTab<R, L>::size;
-    });
-    // The register-FFT row kernels move the spectrum of consecutive rows as 16-byte
-    // pieces of the column-major X[c][kx][j]: in FP32 a piece is two rows, so the
-    // column stride ny must be even for every piece to start on a 16-byte boundary.
-    c.ok_row = okr && c.smem_row <= kSmemMax && (sizeof(R) == 8 || ny % 2 == 0);
-    c.ok_col = okc && c.smem_col + kStaticSmemCol <= kSmemMax;
-    c.ok = c.ok_row && c.ok_col;
+    for (int v = 0; v < 2; ++v) {
+        bool okr = dispatch_LV<R>(nx, v, [&](auto LC, auto VC) {
+            constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+            c.T[v] = RowCfg<R, L, V>::T;
+            c.row_threads[v] = RowCfg<R, L, V>::THREADS;
+            c.smem_row[v] = RowCfg<R, L, V>::SMEM;
+            c.twp_row_size[v] = TwTab<R, L, V>::size;
+        });
+        bool okc = dispatch_LV<R>(ny, v, [&](auto LC, auto VC) {
+            constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+            c.NC[v] = ColCfg<R, L, V>::NC;
+            c.col_threads[v] = ColCfg<R, L, V>::THREADS;
+            c.smem_col[v] = ColCfg<R, L, V>::SMEM;
+            c.twp_col_size[v] = TwTab<R, L, V>::size;
+        });
+        // The register-FFT row kernels move the spectrum of consecutive rows as 16-byte
+        // pieces of the column-major X[c][kx][j]: in FP32 a piece is two rows, so the
+        // column stride ny must be even for every piece to start on a 16-byte boundary.
+        c.ok_row[v] = okr && c.smem_row[v] <= kSmemMax && (sizeof(R) == 8 || ny % 2 == 0);
+        c.ok_col[v] = okc && c.smem_col[v] + kStaticSmemCol <= kSmemMax;
+    }
     return c;
 }
 
 template <typename R>
-cudaError_t build_pass_tables(void* out_row, int nx, void* out_col, int ny, cudaStream_t s) {
+cudaError_t build_pass_tables(void* out, int L_, int v, cudaStream_t s) {
     cudaError_t err = cudaSuccess;
-    dispatch_L<R>(nx, [&](auto LC) {
-        constexpr int L = decltype(LC)::value;
-        if (TwTab<R, L>::size > 0) {
-            k_pass_tables<R, L><<<(TwTab<R, L>::size + 255) / 256, 256, 0, s>>>(reinterpret_cast<cx<R>*>(out_row));
-            err = cudaGetLastError();
-        }
-    });
-    if (err != cudaSuccess) return err;
-    dispatch_L<R>(ny, [&](auto LC) {
-        constexpr int L = decltype(LC)::value;
-        if (TwTab<R, L>::size > 0) {
-            k_pass_tables<R, L><<<(TwTab<R, L>::size + 255) / 256, 256, 0, s>>>(reinterpret_cast<cx<R>*>(out_col));
+    dispatch_LV<R>(L_, v, [&](auto LC, auto VC) {
+        constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+        if (TwTab<R, L, V>::size > 0) {
+            k_pass_tables<R, L, V><<<(TwTab<R, L, V>::size + 255) / 256, 256, 0, s>>>(reinterpret_cast<cx<R>*>(out));
             err = cudaGetLastError();
         }
     });
@@ -105,41 +115,28 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_col);
     if (e != cudaSuccess) return e;
-    // fast kernels: every instantiation whose shared memory fits
-    auto set_all = [&](auto LC) {
-        constexpr int L = decltype(LC)::value;
-        if (RowCfg<R, L>::SMEM <= kSmemMax) {
-            cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)RowCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_row_inverse_fast<R, L, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)RowCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_row_inverse_fast<R, L, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)RowCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)RowCfg<R, L>::SMEM);
+    // fast kernels: every instantiation whose shared memory fits; the whole unified
+    // L1/shared array as shared memory, so that occupancy is bounded by registers
+    // and the blocks' own shared memory only
+    auto set_all = [&](auto LC, auto VC) {
+        constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+        auto both = [](const void* f, int bytes) {
+            cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        };
+        if constexpr (RowCfg<R, L, V>::SMEM <= kSmemMax) {
+            constexpr int sm = (int)RowCfg<R, L, V>::SMEM;
+            both((const void*)k_row_forward_fast<R, L, V>, sm);
+            both((const void*)k_row_inverse_fast<R, L, 0, V>, sm);
+            both((const void*)k_row_inverse_fast<R, L, 1, V>, sm);
+            both((const void*)k_row_inverse_fast<R, L, 2, V>, sm);
+            both((const void*)k_row_fused<R, L, V>, sm);
         }
-        if (RowCfg<R, L>::SMEM <= kSmemMax) {
-            cudaFuncSetAttribute(k_row_fused<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)RowCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_row_fused<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        }
-        if (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax)
-            cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ColCfg<R, L>::SMEM);
-        if (ColDirectCfg<R, L>::SMEM <= kSmemMax) {
-            cudaFuncSetAttribute(k_column_direct<R, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ColDirectCfg<R, L>::SMEM);
-            cudaFuncSetAttribute(k_column_direct<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        }
-        // the whole unified L1/shared array as shared memory, so that occupancy is
-        // bounded by registers and the blocks' own shared memory only
-        cudaFuncSetAttribute(k_row_forward_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(k_row_inverse_fast<R, L, 0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(k_row_inverse_fast<R, L, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(k_row_inverse_fast<R, L, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(k_column_fast<R, L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if constexpr (ColCfg<R, L, V>::SMEM + kStaticSmemCol <= kSmemMax)
+            both((const void*)k_column_fast<R, L, V>, (int)ColCfg<R, L, V>::SMEM);
     };
-    for (int L : {16, 32, 64, 128, 256, 512, 1024, 2048}) dispatch_L<R>(L, set_all);
+    for (int L : {16, 32, 64, 128, 256, 512, 1024, 2048})
+        for (int v = 0; v < 2; ++v) dispatch_LV<R>(L, v, set_all);
     return cudaGetLastError();
 }
 
@@ -148,20 +145,20 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
     int count = 0;
     if (which == 0 || which == 2) {
         if (g.fast_row) {
-            dispatch_L<R>(g.fast_row, [&](auto LC) {
-                constexpr int L = decltype(LC)::value;
-                if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
-                    using C = RowCfg<R, L>;
+            dispatch_LV<R>(g.fast_row, g.row_var, [&](auto LC, auto VC) {
+                constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+                if constexpr (RowCfg<R, L, V>::SMEM <= kSmemMax) {
+                    using C = RowCfg<R, L, V>;
                     if (which == 0) {
-                        k_row_forward_fast<R, L><<<g.grid_row, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
-                                                                                        g.n_row_items, spec);
+                        k_row_forward_fast<R, L, V><<<g.grid_row, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
+                                                                                           g.n_row_items, spec);
                         ++count;
                     } else if (lean_epilogue(spec) || lean_err45_epilogue(spec)) {
                         // transform only, then the torque epilogue as a streaming kernel
                         constexpr int CPI = C::T * L;
                         const long long cells = (long long)g.n_row_items * CPI;
-                        k_row_inverse_fast<R, L, 1><<<g.grid_rinv, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
-                                                                                            g.n_row_items, spec);
+                        k_row_inverse_fast<R, L, 1, V><<<g.grid_rinv, C::THREADS, C::SMEM, s>>>(
+                            g.films, g.row_items, g.n_row_items, spec);
                         if (lean_err45_epilogue(spec))
                             k_stage_torque<R, true><<<stage_grid(cells), 256, 0, s>>>(g.films, g.row_items,
                                                                                         g.n_row_items, CPI, spec);
@@ -170,12 +167,12 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
                                                                                          g.n_row_items, CPI, spec);
                         count += 2;
                     } else if (spec.rhs == RHS_MINIMIZE) {
-                        k_row_inverse_fast<R, L, 2><<<g.grid_rfull, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
-                                                                                             g.n_row_items, spec);
+                        k_row_inverse_fast<R, L, 2, V><<<g.grid_rfull, C::THREADS, C::SMEM, s>>>(
+                            g.films, g.row_items, g.n_row_items, spec);
                         ++count;
                     } else {
-                        k_row_inverse_fast<R, L, 0><<<g.grid_rfull, C::THREADS, C::SMEM, s>>>(g.films, g.row_items,
-                                                                                             g.n_row_items, spec);
+                        k_row_inverse_fast<R, L, 0, V><<<g.grid_rfull, C::THREADS, C::SMEM, s>>>(
+                            g.films, g.row_items, g.n_row_items, spec);
                         ++count;
                     }
                 }
@@ -194,16 +191,11 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
         }
     } else {
         if (g.fast_col) {
-            dispatch_L<R>(g.fast_col, [&](auto LC) {
-                constexpr int L = decltype(LC)::value;
-                if (g.col_direct) {
-                    if constexpr (ColDirectCfg<R, L>::SMEM <= kSmemMax)
-                        k_column_direct<R, L><<<g.grid_col, ColCfg<R, L>::THREADS, ColDirectCfg<R, L>::SMEM, s>>>(
-                            g.films, g.col_items, g.n_col_items, spec);
-                } else if constexpr (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax) {
-                    k_column_fast<R, L><<<g.grid_col, ColCfg<R, L>::THREADS, ColCfg<R, L>::SMEM, s>>>(
+            dispatch_LV<R>(g.fast_col, g.col_var, [&](auto LC, auto VC) {
+                constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+                if constexpr (ColCfg<R, L, V>::SMEM + kStaticSmemCol <= kSmemMax)
+                    k_column_fast<R, L, V><<<g.grid_col, ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::SMEM, s>>>(
                         g.films, g.col_items, g.n_col_items, spec);
-                }
             });
         } else {
             k_column<R><<<g.grid_col, 256, g.smem_col, s>>>(g.films, g.col_items, g.n_col_items, spec);
@@ -222,11 +214,12 @@ bool can_fuse(const EvalSpec& si, const EvalSpec& sf, const LaunchGeom& g) {
 
 template <typename R>
 cudaError_t launch_fused(const EvalSpec& si, const EvalSpec& sf, const LaunchGeom& g, cudaStream_t s, int* nk) {
-    dispatch_L<R>(g.fast_row, [&](auto LC) {
-        constexpr int L = decltype(LC)::value;
-        if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
-            using C = RowCfg<R, L>;
-            k_row_fused<R, L><<<g.grid_fused, C::THREADS, C::SMEM, s>>>(g.films, g.row_items, g.n_row_items, si, sf);
+    dispatch_LV<R>(g.fast_row, g.row_var, [&](auto LC, auto VC) {
+        constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+        if constexpr (RowCfg<R, L, V>::SMEM <= kSmemMax) {
+            using C = RowCfg<R, L, V>;
+            k_row_fused<R, L, V><<<g.grid_fused, C::THREADS, C::SMEM, s>>>(g.films, g.row_items, g.n_row_items, si,
+                                                                           sf);
         }
     });
     if (nk) *nk += 1;
@@ -245,52 +238,44 @@ cudaError_t launch_eval(const EvalSpec& spec, const LaunchGeom& g, cudaStream_t 
 }
 
 template <typename R>
-void fast_occupancy(int nx, int ny, bool col_direct, int* fwd_blocks_per_sm, int* inv_blocks_per_sm,
+void fast_occupancy(int nx, int ny, int row_var, int col_var, int* fwd_blocks_per_sm, int* inv_blocks_per_sm,
                     int* full_blocks_per_sm, int* fused_blocks_per_sm, int* col_blocks_per_sm) {
     *fwd_blocks_per_sm = *inv_blocks_per_sm = *full_blocks_per_sm = *fused_blocks_per_sm = *col_blocks_per_sm = 1;
-    dispatch_L<R>(nx, [&](auto LC) {
-        constexpr int L = decltype(LC)::value;
-        if constexpr (RowCfg<R, L>::SMEM <= kSmemMax) {
-            int a = 1, b = 1, c = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_row_forward_fast<R, L>, RowCfg<R, L>::THREADS,
-                                                          RowCfg<R, L>::SMEM);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_row_inverse_fast<R, L, 1>, RowCfg<R, L>::THREADS,
-                                                          RowCfg<R, L>::SMEM);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_row_inverse_fast<R, L, 0>, RowCfg<R, L>::THREADS,
-                                                          RowCfg<R, L>::SMEM);
+    dispatch_LV<R>(nx, row_var, [&](auto LC, auto VC) {
+        constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+        if constexpr (RowCfg<R, L, V>::SMEM <= kSmemMax) {
+            using C = RowCfg<R, L, V>;
+            int a = 1, b = 1, c = 1, d = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_row_forward_fast<R, L, V>, C::THREADS, C::SMEM);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_row_inverse_fast<R, L, 1, V>, C::THREADS, C::SMEM);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_row_inverse_fast<R, L, 0, V>, C::THREADS, C::SMEM);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_row_fused<R, L, V>, C::THREADS, C::SMEM);
             *fwd_blocks_per_sm = std::max(1, a);
             *inv_blocks_per_sm = std::max(1, b);
             *full_blocks_per_sm = std::max(1, c);
-            int d = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, k_row_fused<R, L>, RowCfg<R, L>::THREADS,
-                                                          RowCfg<R, L>::SMEM);
             *fused_blocks_per_sm = std::max(1, d);
         }
     });
-    dispatch_L<R>(ny, [&](auto LC) {
-        constexpr int L = decltype(LC)::value;
-        if constexpr (ColCfg<R, L>::SMEM + kStaticSmemCol <= kSmemMax) {
+    dispatch_LV<R>(ny, col_var, [&](auto LC, auto VC) {
+        constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
+        if constexpr (ColCfg<R, L, V>::SMEM + kStaticSmemCol <= kSmemMax) {
             int a = 1;
-            if (col_direct)
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_direct<R, L>, ColCfg<R, L>::THREADS,
-                                                              ColDirectCfg<R, L>::SMEM);
-            else
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L>, ColCfg<R, L>::THREADS,
-                                                              ColCfg<R, L>::SMEM);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L, V>, ColCfg<R, L, V>::THREADS,
+                                                          ColCfg<R, L, V>::SMEM);
             *col_blocks_per_sm = std::max(1, a);
         }
     });
 }
-template void fast_occupancy<float>(int, int, bool, int*, int*, int*, int*, int*);
-template void fast_occupancy<double>(int, int, bool, int*, int*, int*, int*, int*);
-template cudaError_t launch_fused<float>(const EvalSpec&, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
-template cudaError_t launch_fused<double>(const EvalSpec&, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
+template void fast_occupancy<float>(int, int, int, int, int*, int*, int*, int*, int*);
+template void fast_occupancy<double>(int, int, int, int, int*, int*, int*, int*, int*);
 template FastCfg fast_config<float>(int, int);
 template FastCfg fast_config<double>(int, int);
-template cudaError_t build_pass_tables<float>(void*, int, void*, int, cudaStream_t);
-template cudaError_t build_pass_tables<double>(void*, int, void*, int, cudaStream_t);
+template cudaError_t build_pass_tables<float>(void*, int, int, cudaStream_t);
+template cudaError_t build_pass_tables<double>(void*, int, int, cudaStream_t);
 template cudaError_t launch_one<float>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
 template cudaError_t launch_one<double>(int, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
+template cudaError_t launch_fused<float>(const EvalSpec&, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
+template cudaError_t launch_fused<double>(const EvalSpec&, const EvalSpec&, const LaunchGeom&, cudaStream_t, int*);
 template cudaError_t prepare_eval_kernels<float>(size_t, size_t);
 template cudaError_t prepare_eval_kernels<double>(size_t, size_t);
 template cudaError_t launch_eval<float>(const EvalSpec&, const LaunchGeom&, cudaStream_t);

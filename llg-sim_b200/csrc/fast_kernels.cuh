@@ -12,9 +12,9 @@ namespace llg {
 
 // Row passes: T rows per block; signals: T packed xy rows and T/2 packed z
 // row pairs, each as an even-bin and an odd-bin transform (s = 2g + parity).
-template <typename R, int L>
+template <typename R, int L, int V = 0>
 struct RowCfg {
-    using P = FPlan<R, L>;
+    using P = FPlan<R, L, V>;
     static constexpr int G = P::G, E = P::E;
     static constexpr int T = (64 / G) < 2 ? 2 : 64 / G;
     static constexpr int NGRP = T + T / 2;
@@ -23,9 +23,12 @@ struct RowCfg {
     // register caps: one resident block at least (REGCAP), three resident
     // 192-thread blocks per SM for the FP32 forward and lean inverse passes (MAXREG)
     static constexpr int REGCAP = (65536 / THREADS) / 8 * 8 > 255 ? 255 : (65536 / THREADS) / 8 * 8;
-    static constexpr int MAXREG = (sizeof(R) == 4 && THREADS <= 192) ? 112 : REGCAP;
-    static constexpr int BUF = Pad<R, L>::size;
-    static constexpr int SMEM_CX = NSIG * BUF + TwTab<R, L>::size + L;
+    // plan 1 (half the registers per thread) is capped for two resident blocks
+    static constexpr int MAXREG = V == 1 ? ((65536 / (2 * THREADS)) / 8 * 8 > REGCAP ? REGCAP
+                                                                                     : (65536 / (2 * THREADS)) / 8 * 8)
+                                         : (sizeof(R) == 4 && THREADS <= 192) ? 112 : REGCAP;
+    static constexpr int BUF = Pad<R, L, V>::size;
+    static constexpr int SMEM_CX = NSIG * BUF + TwTab<R, L, V>::size + L;
     static constexpr size_t SMEM = sizeof(cx<R>) * (size_t)SMEM_CX;
 };
 
@@ -34,20 +37,21 @@ struct RowCfg {
 // tables and pre-twiddles, and the staging areas that the bulk copies of the
 // next item's spectrum columns (Xst, [3][NC][L]) and folded kernel columns
 // (Kst, [NC][L+1]) land in while the current item is transformed.
-template <typename R, int L>
+template <typename R, int L, int V = 0>
 struct ColCfg {
-    using P = FPlan<R, L>;
+    using P = FPlan<R, L, V>;
     static constexpr int G = P::G, E = P::E;
     static constexpr int NC = (32 / G) < 1 ? 1 : 32 / G;
     static constexpr int NSIG = 6 * NC;
     static constexpr int THREADS = NSIG * G;
-    static constexpr int BUF = Pad<R, L>::size;
+    static constexpr int BUF = Pad<R, L, V>::size;
     static constexpr size_t al16(size_t b) { return (b + 15) / 16 * 16; }
     static constexpr size_t OFF_TW = al16(sizeof(cx<R>) * (size_t)NSIG * BUF);
-    static constexpr size_t OFF_PRE = al16(OFF_TW + sizeof(cx<R>) * (size_t)TwTab<R, L>::size);
+    static constexpr size_t OFF_PRE = al16(OFF_TW + sizeof(cx<R>) * (size_t)TwTab<R, L, V>::size);
     static constexpr size_t OFF_XST = al16(OFF_PRE + sizeof(cx<R>) * (size_t)L);
     static constexpr size_t OFF_KST = al16(OFF_XST + sizeof(cx<R>) * 3 * (size_t)NC * L);
     static constexpr size_t SMEM = al16(OFF_KST + sizeof(r4<R>) * (size_t)NC * (L + 1));
+    static constexpr int MINB = V == 1 ? 2 : 1;   // plan 1: registers capped for two resident blocks
 };
 
 template <typename R>
@@ -58,17 +62,17 @@ __device__ __forceinline__ void load_tables(cx<R>* twp, const cx<R>* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-template <typename R, int L>
-__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((RowCfg<R, L>::MAXREG)) k_row_forward_fast(const FilmDev* __restrict__ films,
+template <typename R, int L, int V>
+__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<R, L, V>::MAXREG)) k_row_forward_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
                                                                             int nitems, EvalSpec spec) {
-    using C = RowCfg<R, L>;
-    using FFT = GroupFFT<R, L, false>;
+    using C = RowCfg<R, L, V>;
+    using FFT = GroupFFT<R, L, false, V>;
     constexpr int G = C::G, E = C::E, T = C::T, BUF = C::BUF;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R>* buf = reinterpret_cast<cx<R>*>(smem_raw);
     cx<R>* twp = buf + C::NSIG * BUF;
-    cx<R>* pre = twp + TwTab<R, L>::size;
+    cx<R>* pre = twp + TwTab<R, L, V>::size;
     const int tid = threadIdx.x, s = tid / G, t = tid % G, g = s >> 1, par = s & 1;
     bool tables = false;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -78,7 +82,7 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((RowCfg<R, 
         if (skip_item(spec, st)) continue;
         const bool do_fft = spec.demag && F.demag_mat;
         if (do_fft && !tables) {
-            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_row), TwTab<R, L>::size, pre,
+            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_row[V]), TwTab<R, L, V>::size, pre,
                            reinterpret_cast<const cx<R>*>(F.tw_row), L);
             tables = true;
         }
@@ -232,10 +236,10 @@ __device__ __forceinline__ bool col_item_has(const FilmDev* __restrict__ films, 
     return it < nitems && spec.demag && films[items[it].film].demag_mat;
 }
 
-template <typename R, int L>
+template <typename R, int L, int V>
 __device__ __forceinline__ void col_issue_x(const FilmDev* __restrict__ films, const WorkItem* __restrict__ items,
                                             int it, cx<R>* xst, uint64_t* bar) {
-    using C = ColCfg<R, L>;
+    using C = ColCfg<R, L, V>;
     const WorkItem w = items[it];
     const FilmDev& F = films[w.film];
     const int K1 = F.nx + 1, kx0 = w.blk * C::NC;
@@ -247,10 +251,10 @@ __device__ __forceinline__ void col_issue_x(const FilmDev* __restrict__ films, c
     for (int c = 0; c < 3; ++c) bulk_copy_g2s(xst + (size_t)c * C::NC * L, X + ((size_t)c * K1 + kx0) * L, bytes, bar);
 }
 
-template <typename R, int L>
+template <typename R, int L, int V>
 __device__ __forceinline__ void col_issue_k(const FilmDev* __restrict__ films, const WorkItem* __restrict__ items,
                                             int it, r4<R>* kst, uint64_t* bar) {
-    using C = ColCfg<R, L>;
+    using C = ColCfg<R, L, V>;
     const WorkItem w = items[it];
     const FilmDev& F = films[w.film];
     const int K1 = F.nx + 1, kx0 = w.blk * C::NC;
@@ -260,13 +264,13 @@ __device__ __forceinline__ void col_issue_k(const FilmDev* __restrict__ films, c
     bulk_copy_g2s(kst, reinterpret_cast<const r4<R>*>(F.Khat) + (size_t)kx0 * (L + 1), bytes, bar);
 }
 
-template <typename R, int L>
-__global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const FilmDev* __restrict__ films,
+template <typename R, int L, int V>
+__global__ void __launch_bounds__(ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::MINB) k_column_fast(const FilmDev* __restrict__ films,
                                                                        const WorkItem* __restrict__ items, int nitems,
                                                                        EvalSpec spec) {
-    using C = ColCfg<R, L>;
-    using FF = GroupFFT<R, L, false>;
-    using FI = GroupFFT<R, L, true>;
+    using C = ColCfg<R, L, V>;
+    using FF = GroupFFT<R, L, false, V>;
+    using FI = GroupFFT<R, L, true, V>;
     constexpr int G = C::G, E = C::E, BUF = C::BUF, NC = C::NC;
     constexpr int ny = L, L2 = 2 * L;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -288,8 +292,8 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
     __syncthreads();
     const int it0 = blockIdx.x;
     if (tid == 0 && col_item_has<R, L>(films, items, nitems, spec, it0)) {
-        col_issue_x<R, L>(films, items, it0, xst, &bars[0]);
-        col_issue_k<R, L>(films, items, it0, kst, &bars[1]);
+        col_issue_x<R, L, V>(films, items, it0, xst, &bars[0]);
+        col_issue_k<R, L, V>(films, items, it0, kst, &bars[1]);
     }
     uint32_t phase = 0;
     bool tables = false;
@@ -300,15 +304,15 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
         if (!has) {   // nothing was fetched for this item (uniform over the block)
             if (tid == 0 && has_next) {
                 fence_async_smem();
-                col_issue_x<R, L>(films, items, nxt, xst, &bars[0]);
-                col_issue_k<R, L>(films, items, nxt, kst, &bars[1]);
+                col_issue_x<R, L, V>(films, items, nxt, xst, &bars[0]);
+                col_issue_k<R, L, V>(films, items, nxt, kst, &bars[1]);
             }
             continue;
         }
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
         if (!tables) {
-            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_col), TwTab<R, L>::size, pre,
+            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_col[V]), TwTab<R, L, V>::size, pre,
                            reinterpret_cast<const cx<R>*>(F.tw_col), L);
             tables = true;
         }
@@ -338,7 +342,7 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
         __syncthreads();   // staged spectrum consumed
         if (tid == 0 && has_next) {
             fence_async_smem();
-            col_issue_x<R, L>(films, items, nxt, xst, &bars[0]);
+            col_issue_x<R, L, V>(films, items, nxt, xst, &bars[0]);
         }
         if (run) {
             FF::run(v, t, buf + s * BUF, twp);
@@ -376,7 +380,7 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
         __syncthreads();   // products formed: the signal buffers and staged kernel are free
         if (tid == 0 && has_next) {
             fence_async_smem();
-            col_issue_k<R, L>(films, items, nxt, kst, &bars[1]);
+            col_issue_k<R, L, V>(films, items, nxt, kst, &bars[1]);
         }
         if (run) {
             FI::run(v, t, buf + s * BUF, twp);
@@ -400,122 +404,20 @@ __global__ void __launch_bounds__(ColCfg<R, L>::THREADS) k_column_fast(const Fil
 }
 
 // ---------------------------------------------------------------------------
-// Column pass without staging: the same transforms and kernel product as
-// k_column_fast, but each thread loads its E spectrum values straight from HBM /
-// L2 into registers (all loads of an item in flight at once, coalesced across the
-// transform group) and the kernel planes through L1.  Without the 40 KB staging
-// area three blocks fit per SM instead of two.
-template <typename R, int L>
-struct ColDirectCfg {
-    using C = ColCfg<R, L>;
-    static constexpr size_t SMEM = C::OFF_XST;
-};
-
-template <typename R, int L>
-__global__ void __launch_bounds__(ColCfg<R, L>::THREADS, (sizeof(R) == 4 && ColCfg<R, L>::THREADS <= 192) ? 3 : 1)
-    k_column_direct(const FilmDev* __restrict__ films,
-                                                                         const WorkItem* __restrict__ items,
-                                                                         int nitems, EvalSpec spec) {
-    using C = ColCfg<R, L>;
-    using FF = GroupFFT<R, L, false>;
-    using FI = GroupFFT<R, L, true>;
-    constexpr int G = C::G, E = C::E, BUF = C::BUF, NC = C::NC;
-    constexpr int ny = L, L2 = 2 * L;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<R>* buf = reinterpret_cast<cx<R>*>(smem_raw);
-    cx<R>* twp = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_TW);
-    cx<R>* pre = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_PRE);
-    const int tid = threadIdx.x, s = tid / G, t = tid % G;
-    const int cl = s / 6, comp = (s % 6) >> 1, par = s & 1;
-    bool tables = false;
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-        const WorkItem w = items[it];
-        const FilmDev& F = films[w.film];
-        if (!(spec.demag && F.demag_mat) || skip_item(spec, F.st)) continue;   // uniform over the block
-        if (!tables) {
-            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_col), TwTab<R, L>::size, pre,
-                           reinterpret_cast<const cx<R>*>(F.tw_col), L);
-            tables = true;
-            __syncthreads();
-        }
-        const int K1 = F.nx + 1;
-        const int kx = w.blk * NC + cl;
-        const bool valid = kx < K1;
-        cx<R>* __restrict__ X = reinterpret_cast<cx<R>*>(F.X);
-        const cx<R>* __restrict__ col = X + ((size_t)comp * K1 + (valid ? kx : 0)) * ny;
-        cx<R> v[E];
-#pragma unroll
-        for (int r = 0; r < E; ++r) v[r] = valid ? col[t + G * r] : mkc((R)0, (R)0);
-#pragma unroll
-        for (int r = 0; r < E; ++r)
-            if (par) v[r] = cmul(v[r], pre[t + G * r]);
-        FF::run(v, t, buf + s * BUF, twp);
-        group_sync<G>();
-#pragma unroll
-        for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FF::out_index(t, i))] = v[i];
-        __syncthreads();   // all components of the column transformed
-        const r4<R>* __restrict__ kc = reinterpret_cast<const r4<R>*>(F.Khat) + (size_t)(valid ? kx : 0) * (L + 1);
-        const cx<R>* sx = buf + (6 * cl + 0 + par) * BUF;
-        const cx<R>* sy = buf + (6 * cl + 2 + par) * BUF;
-        const cx<R>* sz = buf + (6 * cl + 4 + par) * BUF;
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-            const int kk = t + G * r;
-            const int ky = 2 * kk + par;
-            // the kernel spectrum is even in ky except Kxy, which is odd
-            const bool up = ky > ny;
-            const r4<R> K = kc[up ? L2 - ky : ky];
-            const R kxy = up ? -K.y : K.y;
-            const int pi = padi<E>(kk);
-            cx<R> out;
-            if (comp == 0) {
-                const cx<R> Mx = sx[pi], My = sy[pi];
-                out = mkc(K.x * Mx.re + kxy * My.re, K.x * Mx.im + kxy * My.im);
-            } else if (comp == 1) {
-                const cx<R> Mx = sx[pi], My = sy[pi];
-                out = mkc(kxy * Mx.re + K.z * My.re, kxy * Mx.im + K.z * My.im);
-            } else {
-                const cx<R> Mz = sz[pi];
-                out = mkc(K.w * Mz.re, K.w * Mz.im);
-            }
-            v[r] = out;
-        }
-        __syncthreads();   // products formed: the signal buffers are free
-        FI::run(v, t, buf + s * BUF, twp);
-        group_sync<G>();
-        if (par) {
-#pragma unroll
-            for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FI::out_index(t, i))] = v[i];
-        }
-        __syncthreads();   // odd-bin results visible to the even-bin groups
-        if (!par && valid) {
-            const cx<R>* ob = buf + (s + 1) * BUF;
-            cx<R>* __restrict__ dst = X + ((size_t)comp * K1 + kx) * ny;
-#pragma unroll
-            for (int i = 0; i < E; ++i) {
-                const int nn = FI::out_index(t, i);
-                dst[nn] = v[i] + cmulc(ob[padi<E>(nn)], pre[nn]);
-            }
-        }
-        __syncthreads();   // buffers reused by the next item
-    }
-}
-
-// ---------------------------------------------------------------------------
 // MODE 0: full epilogue; 1: no epilogue, the demag field is written to the film's
 // bdem planes for k_stage_torque; 2: the minimiser epilogue (RHS_MINIMIZE).
-template <typename R, int L, int MODE>
-__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((MODE == 1 ? RowCfg<R, L>::MAXREG : RowCfg<R, L>::REGCAP)) k_row_inverse_fast(const FilmDev* __restrict__ films,
+template <typename R, int L, int MODE, int V>
+__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((MODE == 1 ? RowCfg<R, L, V>::MAXREG : RowCfg<R, L, V>::REGCAP)) k_row_inverse_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
                                                                             int nitems, EvalSpec spec) {
-    using C = RowCfg<R, L>;
-    using FI = GroupFFT<R, L, true>;
+    using C = RowCfg<R, L, V>;
+    using FI = GroupFFT<R, L, true, V>;
     constexpr int G = C::G, E = C::E, T = C::T, BUF = C::BUF;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sm_red[32 * RED_NSLOT];
     cx<R>* buf = reinterpret_cast<cx<R>*>(smem_raw);
     cx<R>* twp = buf + C::NSIG * BUF;
-    cx<R>* pre = twp + TwTab<R, L>::size;
+    cx<R>* pre = twp + TwTab<R, L, V>::size;
     const int tid = threadIdx.x, s = tid / G, t = tid % G, g = s >> 1, par = s & 1;
     bool tables = false;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -525,7 +427,7 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((MODE == 1 
         if (skip_item(spec, st)) continue;
         const bool do_fft = spec.demag && F.demag_mat;
         if (do_fft && !tables) {
-            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_row), TwTab<R, L>::size, pre,
+            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_row[V]), TwTab<R, L, V>::size, pre,
                            reinterpret_cast<const cx<R>*>(F.tw_row), L);
             tables = true;
             __syncthreads();
@@ -623,10 +525,10 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((MODE == 1 
 }
 
 // Pass twiddle tables [r][k] for GroupFFT<R, L>.
-template <typename R, int L>
+template <typename R, int L, int V>
 __global__ void k_pass_tables(cx<R>* out) {
-    using P = FPlan<R, L>;
-    using TT = TwTab<R, L>;
+    using P = FPlan<R, L, V>;
+    using TT = TwTab<R, L, V>;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < TT::size; e += gridDim.x * blockDim.x) {
         long long k, r, N;
         if (e < TT::size1) {

@@ -117,32 +117,49 @@ struct RegDFT {
     }
 };
 
-// Pass plans.  E = registers (complex) per thread = first radix.
-template <typename R, int L>
-struct FPlan;
-#define LLG_PLAN(RT, LL, EE, NPASS, R1, R2)                          \
+// Pass plans.  E = registers (complex) per thread = first radix; later passes
+// have radices RAD1, RAD2 dividing E.  V = 0 is the default plan of a length;
+// V = 1 an alternative with half the registers per thread and twice the threads
+// per transform (ok = false where a length has none), chosen per launch segment by
+// the engine's autotuner.
+template <typename R, int L, int V = 0>
+struct FPlan {
+    static constexpr bool ok = false;
+    static constexpr int E = 1, NP = 1, G = L, RAD1 = 1, RAD2 = 1;
+};
+#define LLG_PLAN(RT, LL, VV, EE, NPASS, R1, R2)                      \
     template <>                                                      \
-    struct FPlan<RT, LL> {                                           \
+    struct FPlan<RT, LL, VV> {                                       \
+        static constexpr bool ok = true;                             \
         static constexpr int E = EE, NP = NPASS, G = LL / EE;        \
         static constexpr int RAD1 = R1, RAD2 = R2;                   \
     };
-//      type    L     E   NP  R1  R2
-LLG_PLAN(float, 16, 16, 1, 1, 1)
-LLG_PLAN(float, 32, 8, 2, 4, 1)
-LLG_PLAN(float, 64, 8, 2, 8, 1)
-LLG_PLAN(float, 128, 16, 2, 8, 1)
-LLG_PLAN(float, 256, 16, 2, 16, 1)
-LLG_PLAN(float, 512, 32, 2, 16, 1)
-LLG_PLAN(float, 1024, 32, 2, 32, 1)
-LLG_PLAN(float, 2048, 32, 3, 32, 2)
-LLG_PLAN(double, 16, 16, 1, 1, 1)
-LLG_PLAN(double, 32, 8, 2, 4, 1)
-LLG_PLAN(double, 64, 8, 2, 8, 1)
-LLG_PLAN(double, 128, 16, 2, 8, 1)
-LLG_PLAN(double, 256, 16, 2, 16, 1)
-LLG_PLAN(double, 512, 16, 3, 16, 2)
-LLG_PLAN(double, 1024, 16, 3, 16, 4)
-LLG_PLAN(double, 2048, 16, 3, 16, 8)
+//      type    L     V  E   NP  R1  R2
+LLG_PLAN(float, 16, 0, 16, 1, 1, 1)
+LLG_PLAN(float, 32, 0, 8, 2, 4, 1)
+LLG_PLAN(float, 64, 0, 8, 2, 8, 1)
+LLG_PLAN(float, 128, 0, 16, 2, 8, 1)
+LLG_PLAN(float, 256, 0, 16, 2, 16, 1)
+LLG_PLAN(float, 512, 0, 32, 2, 16, 1)
+LLG_PLAN(float, 1024, 0, 32, 2, 32, 1)
+LLG_PLAN(float, 2048, 0, 32, 3, 32, 2)
+LLG_PLAN(double, 16, 0, 16, 1, 1, 1)
+LLG_PLAN(double, 32, 0, 8, 2, 4, 1)
+LLG_PLAN(double, 64, 0, 8, 2, 8, 1)
+LLG_PLAN(double, 128, 0, 16, 2, 8, 1)
+LLG_PLAN(double, 256, 0, 16, 2, 16, 1)
+LLG_PLAN(double, 512, 0, 16, 3, 16, 2)
+LLG_PLAN(double, 1024, 0, 16, 3, 16, 4)
+LLG_PLAN(double, 2048, 0, 16, 3, 16, 8)
+// alternatives: half the registers per thread
+LLG_PLAN(float, 128, 1, 8, 3, 8, 2)
+LLG_PLAN(float, 256, 1, 8, 3, 8, 4)
+LLG_PLAN(float, 512, 1, 16, 3, 16, 2)
+LLG_PLAN(float, 1024, 1, 16, 3, 16, 4)
+LLG_PLAN(float, 2048, 1, 16, 3, 16, 8)
+LLG_PLAN(double, 128, 1, 8, 3, 8, 2)
+LLG_PLAN(double, 256, 1, 8, 3, 8, 4)
+LLG_PLAN(double, 512, 1, 8, 3, 8, 8)
 #undef LLG_PLAN
 
 template <int L>
@@ -157,17 +174,17 @@ template <int E>
 __device__ __forceinline__ int padi(int i) {
     return i + i / E;
 }
-template <typename R, int L>
+template <typename R, int L, int V = 0>
 struct Pad {
-    static constexpr int E = FPlan<R, L>::E;
+    static constexpr int E = FPlan<R, L, V>::E;
     static constexpr int size = L + L / E;  // complex slots per signal buffer
 };
 
 // Twiddle tables of passes 1.. in [r][k] layout: pass with radix Rr and stride
 // ns holds W_{ns*Rr}^{k*r} for r < Rr, k < ns.  Total entries:
-template <typename R, int L>
+template <typename R, int L, int V = 0>
 struct TwTab {
-    using P = FPlan<R, L>;
+    using P = FPlan<R, L, V>;
     static constexpr int ns1 = P::E;
     static constexpr int size1 = P::NP >= 2 ? P::RAD1 * ns1 : 0;
     static constexpr int ns2 = P::E * P::RAD1;
@@ -185,9 +202,9 @@ __device__ __forceinline__ void run_blocks(cx<R> (&v)[E]) {
 
 // One pass p >= 1: read inputs of this thread's butterflies from `buf`,
 // twiddle, DFT in registers.
-template <typename R, int L, bool INV, int RADIX, int NS>
-__device__ __forceinline__ void group_pass(cx<R> (&v)[FPlan<R, L>::E], int t, const cx<R>* buf, const cx<R>* tw) {
-    using P = FPlan<R, L>;
+template <typename R, int L, int V, bool INV, int RADIX, int NS>
+__device__ __forceinline__ void group_pass(cx<R> (&v)[FPlan<R, L, V>::E], int t, const cx<R>* buf, const cx<R>* tw) {
+    using P = FPlan<R, L, V>;
     constexpr int E = P::E, G = P::G, NB = E / RADIX, STRIDE = L / RADIX;
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
@@ -207,9 +224,9 @@ __device__ __forceinline__ void group_pass(cx<R> (&v)[FPlan<R, L>::E], int t, co
 }
 
 // Output index of register v[i] after the pass with radix RADIX and stride NS.
-template <typename R, int L, int RADIX, int NS>
+template <typename R, int L, int V, int RADIX, int NS>
 __device__ __forceinline__ int pass_out_index(int t, int i) {
-    constexpr int G = FPlan<R, L>::G;
+    constexpr int G = FPlan<R, L, V>::G;
     const int u = i / RADIX, q = i % RADIX;
     const int b = t + G * u;
     return (b / NS) * NS * RADIX + (b % NS) + q * NS;
@@ -228,15 +245,15 @@ __device__ __forceinline__ void group_sync() {
 // buffer (only this group touches it inside); `tw` the pass tables.  Every
 // thread of the block must call this the same number of times (it contains
 // group_sync<G>(), a block barrier when G > 32).
-template <typename R, int L, bool INV>
+template <typename R, int L, bool INV, int V = 0>
 struct GroupFFT {
-    using P = FPlan<R, L>;
+    using P = FPlan<R, L, V>;
     static constexpr int E = P::E, G = P::G, NP = P::NP;
 
     __device__ __forceinline__ static int out_index(int t, int i) {
         if constexpr (NP == 1) return t * E + i;
-        else if constexpr (NP == 2) return pass_out_index<R, L, P::RAD1, E>(t, i);
-        else return pass_out_index<R, L, P::RAD2, E * P::RAD1>(t, i);
+        else if constexpr (NP == 2) return pass_out_index<R, L, V, P::RAD1, E>(t, i);
+        else return pass_out_index<R, L, V, P::RAD2, E * P::RAD1>(t, i);
     }
 
     __device__ __forceinline__ static void run(cx<R> (&v)[E], int t, cx<R>* buf, const cx<R>* tw) {
@@ -245,13 +262,13 @@ struct GroupFFT {
 #pragma unroll
             for (int q = 0; q < E; ++q) buf[padi<E>(t * E + q)] = v[q];
             group_sync<G>();
-            group_pass<R, L, INV, P::RAD1, E>(v, t, buf, tw);
+            group_pass<R, L, V, INV, P::RAD1, E>(v, t, buf, tw);
             if constexpr (NP >= 3) {
                 group_sync<G>();
 #pragma unroll
-                for (int i = 0; i < E; ++i) buf[padi<E>(pass_out_index<R, L, P::RAD1, E>(t, i))] = v[i];
+                for (int i = 0; i < E; ++i) buf[padi<E>(pass_out_index<R, L, V, P::RAD1, E>(t, i))] = v[i];
                 group_sync<G>();
-                group_pass<R, L, INV, P::RAD2, E * P::RAD1>(v, t, buf, tw + TwTab<R, L>::size1);
+                group_pass<R, L, V, INV, P::RAD2, E * P::RAD1>(v, t, buf, tw + TwTab<R, L, V>::size1);
             }
         }
     }

@@ -40,18 +40,18 @@ __device__ __forceinline__ void torque_cell(const R* mc, const R* b, R pref, R c
 // si: stage s (inverse half: m_in, k_out, rhs, field terms); sf: stage s+1
 // (forward half: m_in receives m_{s+1}, the combination kidx / a with
 // sf.kidx[sf.nterm - 1] == si.k_out).  Both carry the same request gate.
-template <typename R, int L>
-__global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((RowCfg<R, L>::MAXREG)) k_row_fused(
+template <typename R, int L, int V>
+__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<R, L, V>::MAXREG)) k_row_fused(
     const FilmDev* __restrict__ films, const WorkItem* __restrict__ items, int nitems, EvalSpec si, EvalSpec sf) {
-    using C = RowCfg<R, L>;
-    using FF = GroupFFT<R, L, false>;
-    using FI = GroupFFT<R, L, true>;
+    using C = RowCfg<R, L, V>;
+    using FF = GroupFFT<R, L, false, V>;
+    using FI = GroupFFT<R, L, true, V>;
     constexpr int G = C::G, E = C::E, T = C::T, BUF = C::BUF;
     constexpr int W = Vec16<R>::W, NV = T * L / W;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R>* buf = reinterpret_cast<cx<R>*>(smem_raw);
     cx<R>* twp = buf + C::NSIG * BUF;
-    cx<R>* pre = twp + TwTab<R, L>::size;
+    cx<R>* pre = twp + TwTab<R, L, V>::size;
     const int tid = threadIdx.x, s = tid / G, t = tid % G, g = s >> 1, par = s & 1;
     // signal slot of component c of row r, cell i: x, y of row r in buffer 2r
     // (re, im); z of rows 2p, 2p+1 in buffer 2(T+p) (re, im).  The inverse
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(RowCfg<R, L>::THREADS) __maxnreg__((RowCfg<R, 
         if (skip_item(si, st)) continue;   // uniform over the block
         const bool do_fft = si.demag && F.demag_mat;
         if (do_fft && !tables) {
-            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_row), TwTab<R, L>::size, pre,
+            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_row[V]), TwTab<R, L, V>::size, pre,
                            reinterpret_cast<const cx<R>*>(F.tw_row), L);
             tables = true;
             __syncthreads();

@@ -17,7 +17,9 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/llg_b200.h"
@@ -287,6 +289,7 @@ struct EngineBase {
     virtual int profile_stage(const llg_params* p, int fmask, int reps, double* ms4) = 0;
     virtual long long launch_count() = 0;
     virtual int warm_start(ws::Net* net, const double* bext3n) = 0;
+    virtual int fft_plans(int* rows, int nr, int* cols, int nc) const = 0;
 };
 
 // LLG_B200_GENERIC_FFT=1 selects the generic shared-memory Stockham kernels
@@ -296,6 +299,22 @@ static bool env_flag(const char* name) {
     return e && e[0] == '1';
 }
 static bool force_generic() { return env_flag("LLG_B200_GENERIC_FFT"); }
+
+// A row radix plan is usable in a segment if it exists and keeps the rows per
+// block of plan 0 (the row work items are shared by the plans).
+static bool row_plan_ok(const FastCfg& fc, int v) { return fc.ok_row[v] && fc.T[v] == fc.T[0]; }
+
+// Radix plan chosen per (precision, pass kind, length) for the process.
+static std::mutex g_plan_mutex;
+static std::map<std::tuple<int, int, int>, int> g_plan_cache;
+
+// LLG_B200_FFT_PLAN=0 or 1 fixes the register-FFT radix plan where it exists
+// (-1: the autotuner decides).
+static int forced_plan() {
+    const char* e = std::getenv("LLG_B200_FFT_PLAN");
+    if (e && (e[0] == '0' || e[0] == '1') && e[1] == 0) return e[0] - '0';
+    return -1;
+}
 
 template <typename R>
 struct Engine final : EngineBase {
@@ -338,8 +357,12 @@ struct Engine final : EngineBase {
     // launch segments: films grouped by the row (rseg) / column (cseg) kernel they use,
     // with the resident blocks per SM of each segment's kernels
     std::vector<LaunchGeom> rseg, cseg;
-    std::vector<std::array<int, 4>> rocc;
-    std::vector<int> cocc;
+    // each segment's geometry under radix plan 0 / 1 (where the plan exists) and
+    // the resident blocks per SM of its kernels; the autotuner picks one
+    std::vector<std::array<LaunchGeom, 2>> rseg_alt, cseg_alt;
+    std::vector<std::array<char, 2>> rseg_has, cseg_has;
+    std::vector<std::array<std::array<int, 4>, 2>> rocc;
+    std::vector<std::array<int, 2>> cocc;
 
     int nfilms() const override { return nf; }
     int64_t cells(int f) const override { return grids[f].nx * grids[f].ny; }
@@ -429,8 +452,8 @@ struct Engine final : EngineBase {
         std::vector<char> frow(nf), fcol(nf);
         for (int f = 0; f < nf; ++f) {
             fcs[f] = fast_config<R>((int)g[f].nx, (int)g[f].ny);
-            frow[f] = !gen && fcs[f].ok_row;
-            fcol[f] = !gen && fcs[f].ok_col;
+            frow[f] = !gen && fcs[f].ok_row[0];
+            fcol[f] = !gen && fcs[f].ok_col[0];
         }
         size_t smem_row = 0, smem_col = 0;   // generic kernels
         for (int f = 0; f < nf; ++f) {
@@ -450,8 +473,7 @@ struct Engine final : EngineBase {
         std::map<int, std::vector<WorkItem>> rows_by, cols_by;   // segment key: L of the fast kernel, 0 generic
         for (int f = 0; f < nf; ++f) {
             const int nx = (int)g[f].nx, ny = (int)g[f].ny;
-            const int T = frow[f] ? fcs[f].T : 2;
-            const int NC = fcol[f] ? fcs[f].NC : 1;
+            const int T = frow[f] ? fcs[f].T[0] : 2;
             const int64_t n = (int64_t)nx * ny;
             max_cells = std::max(max_cells, n);
             const size_t plane = sizeof(R) * 3 * (size_t)n;
@@ -512,15 +534,21 @@ struct Engine final : EngineBase {
                 CUDA_TRY(launch_twiddles(tw_col, 2 * ny, sizeof(R) == 8, stream));
                 F.tw_row = tw_row;
                 F.tw_col = tw_col;
-                if (frow[f] || fcol[f]) {
-                    const FastCfg& fc = fcs[f];
-                    void* twp_row;
-                    void* twp_col;
-                    if ((rc = dalloc(&twp_row, sizeof(cx<R>) * (size_t)std::max(fc.twp_row_size, 1)))) return rc;
-                    if ((rc = dalloc(&twp_col, sizeof(cx<R>) * (size_t)std::max(fc.twp_col_size, 1)))) return rc;
-                    CUDA_TRY(build_pass_tables<R>(twp_row, nx, twp_col, ny, stream));
-                    F.twp_row = twp_row;
-                    F.twp_col = twp_col;
+                // register-FFT pass tables of every radix plan the film's lengths have
+                const FastCfg& fc = fcs[f];
+                for (int v = 0; v < 2; ++v) {
+                    if (frow[f] && row_plan_ok(fc, v)) {
+                        void* t;
+                        if ((rc = dalloc(&t, sizeof(cx<R>) * (size_t)std::max(fc.twp_row_size[v], 1)))) return rc;
+                        CUDA_TRY(build_pass_tables<R>(t, nx, v, stream));
+                        F.twp_row[v] = t;
+                    }
+                    if (fcol[f] && fc.ok_col[v]) {
+                        void* t;
+                        if ((rc = dalloc(&t, sizeof(cx<R>) * (size_t)std::max(fc.twp_col_size[v], 1)))) return rc;
+                        CUDA_TRY(build_pass_tables<R>(t, ny, v, stream));
+                        F.twp_col[v] = t;
+                    }
                 }
                 if ((rc = dalloc(&F.X, sizeof(cx<R>) * 3 * (size_t)(nx + 1) * ny))) return rc;
                 if (frow[f] && (rc = dalloc(&F.bdem, plane))) return rc;
@@ -543,9 +571,14 @@ struct Engine final : EngineBase {
                 }
             }
             for (int b = 0; b < F.nblk; ++b) rows_by[frow[f] ? nx : 0].push_back(WorkItem{f, b});
-            const int ncb = (nx + 1 + NC - 1) / NC;
+            // column items per radix plan (a plan fixes the columns per item)
             if (m[f].demag)
-                for (int b = 0; b < ncb; ++b) cols_by[fcol[f] ? ny : 0].push_back(WorkItem{f, b});
+                for (int v = 0; v < 2; ++v) {
+                    if (fcol[f] ? !fcs[f].ok_col[v] : v > 0) continue;
+                    const int NC = fcol[f] ? fcs[f].NC[v] : 1;
+                    const int ncb = (nx + 1 + NC - 1) / NC;
+                    for (int b = 0; b < ncb; ++b) cols_by[fcol[f] ? 2 * ny + v : 0].push_back(WorkItem{f, b});
+                }
         }
         std::vector<WorkItem> rows, cols;
         std::vector<std::pair<int, std::pair<size_t, size_t>>> rspan, cspan;   // key, [offset, count)
@@ -577,7 +610,8 @@ struct Engine final : EngineBase {
         geom.fast_row = 0;
         geom.fast_col = 0;
         geom.fuse_rows = !env_flag("LLG_B200_NO_FUSE");
-        geom.col_direct = !env_flag("LLG_B200_COL_STAGED");
+        geom.row_var = 0;
+        geom.col_var = 0;
         CUDA_TRY(prepare_eval_kernels<R>(smem_row, smem_col));
         {
             // persistent grids: at most one wave of resident blocks looping over the work
@@ -592,29 +626,56 @@ struct Engine final : EngineBase {
             const int gen_r = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_row, 1))));
             const int gen_c = std::min(8, std::max(1, (int)(200 * 1024 / std::max<size_t>(smem_col, 1))));
             for (auto& sp : rspan) {
-                LaunchGeom s = geom;
-                s.row_items = d_row_items + sp.second.first;
-                s.n_row_items = (int)sp.second.second;
-                s.fast_row = sp.first;
-                int fb = gen_r, ib = gen_r, ub = gen_r, zb = 1, cb = 1;
-                if (sp.first) fast_occupancy<R>(sp.first, 0, geom.col_direct, &fb, &ib, &ub, &zb, &cb);
-                s.grid_row = balanced(s.n_row_items, fb);
-                s.grid_rinv = balanced(s.n_row_items, ib);
-                s.grid_rfull = balanced(s.n_row_items, ub);
-                s.grid_fused = balanced(s.n_row_items, zb);
-                rseg.push_back(s);
-                rocc.push_back({fb, ib, ub, zb});
+                std::array<LaunchGeom, 2> alt{};
+                std::array<char, 2> has{0, 0};
+                std::array<std::array<int, 4>, 2> occ{};
+                for (int v = 0; v < 2; ++v) {
+                    const int L = sp.first;
+                    if (L ? !row_plan_ok(fast_config<R>(L, 2), v) : v > 0) continue;
+                    LaunchGeom s = geom;
+                    s.row_items = d_row_items + sp.second.first;
+                    s.n_row_items = (int)sp.second.second;
+                    s.fast_row = L;
+                    s.row_var = v;
+                    int fb = gen_r, ib = gen_r, ub = gen_r, zb = 1, cb = 1;
+                    if (L) fast_occupancy<R>(L, 0, v, 0, &fb, &ib, &ub, &zb, &cb);
+                    s.grid_row = balanced(s.n_row_items, fb);
+                    s.grid_rinv = balanced(s.n_row_items, ib);
+                    s.grid_rfull = balanced(s.n_row_items, ub);
+                    s.grid_fused = balanced(s.n_row_items, zb);
+                    alt[v] = s;
+                    has[v] = 1;
+                    occ[v] = {fb, ib, ub, zb};
+                }
+                rseg.push_back(alt[0]);
+                rseg_alt.push_back(alt);
+                rseg_has.push_back(has);
+                rocc.push_back(occ);
             }
+            // column segments: one per length, with the geometry of each radix plan
+            std::map<int, size_t> col_index;
             for (auto& sp : cspan) {
+                const int L = sp.first ? sp.first / 2 : 0, v = sp.first ? sp.first % 2 : 0;
+                if (!col_index.count(L)) {
+                    col_index[L] = cseg.size();
+                    cseg.push_back(LaunchGeom{});
+                    cseg_alt.push_back({});
+                    cseg_has.push_back({0, 0});
+                    cocc.push_back({1, 1});
+                }
+                const size_t i = col_index[L];
                 LaunchGeom s = geom;
                 s.col_items = d_col_items + sp.second.first;
                 s.n_col_items = (int)sp.second.second;
-                s.fast_col = sp.first;
+                s.fast_col = L;
+                s.col_var = v;
                 int fb = 1, ib = 1, ub = 1, zb = 1, cb = gen_c;
-                if (sp.first) fast_occupancy<R>(0, sp.first, geom.col_direct, &fb, &ib, &ub, &zb, &cb);
+                if (L) fast_occupancy<R>(0, L, 0, v, &fb, &ib, &ub, &zb, &cb);
                 s.grid_col = balanced(s.n_col_items, cb);
-                cseg.push_back(s);
-                cocc.push_back(cb);
+                cseg_alt[i][v] = s;
+                cseg_has[i][v] = 1;
+                cocc[i][v] = cb;
+                if (v == 0) cseg[i] = s;
             }
         }
         if (any_demag && nf == 1) set_l2_window();
@@ -634,9 +695,19 @@ struct Engine final : EngineBase {
     // blocks that need the same number of rounds over the work items, and the full
     // resident wave) on a representative RK45 stage and keep the fastest.  Runs once
     // per engine, on the engine's own buffers, before any state is set.
+    // Radix plans and persistent grids of the register-FFT passes.  For each launch
+    // segment and each radix plan its length has, the candidate grids of every pass
+    // (the fewest blocks that need the same number of rounds over the work items for
+    // 1..occupancy resident blocks per SM, and the full resident wave) are timed on a
+    // representative RK45 stage on the engine's own buffers; a segment keeps the plan
+    // whose passes are fastest in sum, each with its fastest grid.  The plan decides
+    // the arithmetic order of the transforms, so the first decision for a (precision,
+    // pass, length) is kept for the whole process and every engine computes the same
+    // bits; grids do not change results.  LLG_B200_FFT_PLAN=0/1 fixes the plan,
+    // LLG_B200_NO_AUTOTUNE=1 keeps plan 0 and the balanced grids.
     int autotune_grids(int nsm) {
-        if (const char* e = std::getenv("LLG_B200_NO_AUTOTUNE"))
-            if (e[0] == '1') return LLG_OK;
+        const int forced = forced_plan();
+        const bool tuning = !env_flag("LLG_B200_NO_AUTOTUNE");
         int rc;
         if ((rc = set_control(idle_control(), nullptr, nullptr, true))) return rc;
         EvalSpec stage = base_spec(LLG_FIELD_FULL);
@@ -663,7 +734,9 @@ struct Engine final : EngineBase {
             c.erase(std::unique(c.begin(), c.end()), c.end());
             return c;
         };
-        auto tune = [&](int which, const EvalSpec& spec, LaunchGeom& geom, int* grid, int items, int occ) -> int {
+        // best grid of one pass; *best_ms receives its time (4 launches)
+        auto tune = [&](int which, const EvalSpec& spec, LaunchGeom& geom, int* grid, int items, int occ,
+                        float* best_ms) -> int {
             float best = 1e30f;
             int best_g = *grid;
             auto one = [&]() {
@@ -684,21 +757,84 @@ struct Engine final : EngineBase {
                 }
             }
             *grid = best_g;
+            *best_ms = best;
+            return LLG_OK;
+        };
+        auto tune_row = [&](size_t i, int v, float* total) -> int {
+            LaunchGeom& sg = rseg_alt[i][v];
+            const int nr = sg.n_row_items;
+            const auto& oc = rocc[i][v];
+            float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
+            int rc2;
+            if ((rc2 = tune(0, stage, sg, &sg.grid_row, nr, oc[0], &t0))) return rc2;
+            if ((rc2 = tune(2, stage, sg, &sg.grid_rinv, nr, oc[1], &t1))) return rc2;
+            if ((rc2 = tune(2, full, sg, &sg.grid_rfull, nr, oc[2], &t2))) return rc2;
+            if (sg.fast_row && sg.fuse_rows && (rc2 = tune(3, stage, sg, &sg.grid_fused, nr, oc[3], &t3))) return rc2;
+            *total = t0 + t1 + t2 + t3;
+            return LLG_OK;
+        };
+        auto pick = [&](int kind, int L, const std::array<char, 2>& has, auto&& time_plan, int* chosen) -> int {
+            *chosen = 0;
+            if (!L) return LLG_OK;
+            if (forced >= 0) {
+                *chosen = has[forced] ? forced : 0;
+                return LLG_OK;
+            }
+            const std::tuple<int, int, int> key{(int)sizeof(R), kind, L};
+            {
+                std::lock_guard<std::mutex> lock(g_plan_mutex);
+                auto it = g_plan_cache.find(key);
+                if (it != g_plan_cache.end()) {
+                    *chosen = has[it->second] ? it->second : 0;
+                    return LLG_OK;
+                }
+            }
+            if (!tuning) return LLG_OK;
+            float best = 1e30f;
+            for (int v = 0; v < 2; ++v) {
+                if (!has[v]) continue;
+                float t = 0.f;
+                int rc2;
+                if ((rc2 = time_plan(v, &t))) return rc2;
+                if (t < best) {
+                    best = t;
+                    *chosen = v;
+                }
+            }
+            std::lock_guard<std::mutex> lock(g_plan_mutex);
+            g_plan_cache.emplace(key, *chosen);
             return LLG_OK;
         };
         for (size_t i = 0; i < rseg.size(); ++i) {
-            LaunchGeom& sg = rseg[i];
-            const int nr = sg.n_row_items;
-            if ((rc = tune(0, stage, sg, &sg.grid_row, nr, rocc[i][0]))) return rc;
-            if ((rc = tune(2, stage, sg, &sg.grid_rinv, nr, rocc[i][1]))) return rc;
-            if ((rc = tune(2, full, sg, &sg.grid_rfull, nr, rocc[i][2]))) return rc;
-            if (sg.fast_row && sg.fuse_rows && (rc = tune(3, stage, sg, &sg.grid_fused, nr, rocc[i][3]))) return rc;
+            int v = 0;
+            if ((rc = pick(0, rseg[i].fast_row, rseg_has[i],
+                           [&](int pv, float* t) { return tune_row(i, pv, t); }, &v)))
+                return rc;
+            float t = 0.f;
+            if (tuning && (rc = tune_row(i, v, &t))) return rc;   // the kept plan's grids
+            rseg[i] = rseg_alt[i][v];
         }
-        for (size_t i = 0; i < cseg.size(); ++i)
-            if ((rc = tune(1, stage, cseg[i], &cseg[i].grid_col, cseg[i].n_col_items, cocc[i]))) return rc;
+        for (size_t i = 0; i < cseg.size(); ++i) {
+            auto time_col = [&](int pv, float* t) {
+                LaunchGeom& sg = cseg_alt[i][pv];
+                return tune(1, stage, sg, &sg.grid_col, sg.n_col_items, cocc[i][pv], t);
+            };
+            int v = 0;
+            if ((rc = pick(1, cseg[i].fast_col, cseg_has[i], time_col, &v))) return rc;
+            float t = 0.f;
+            if (tuning && (rc = time_col(v, &t))) return rc;
+            cseg[i] = cseg_alt[i][v];
+        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         invalidate_fsal_host();
+        return LLG_OK;
+    }
+
+    // The radix plan each launch segment runs (for reports): [row segments..., column segments...]
+    int fft_plans(int* rows, int nr, int* cols, int nc) const override {
+        for (int i = 0; i < nr && i < (int)rseg.size(); ++i) rows[i] = rseg[i].fast_row ? rseg[i].row_var : -1;
+        for (int i = 0; i < nc && i < (int)cseg.size(); ++i) cols[i] = cseg[i].fast_col ? cseg[i].col_var : -1;
         return LLG_OK;
     }
 
@@ -1781,6 +1917,22 @@ int llg_profile_stage(llg_solver* s, const llg_params* p, int32_t fmask, int32_t
     if (!rc && (!p || !ms4 || reps < 1)) rc = set_error(LLG_ERR_INVALID, "bad argument");
     return rc ? rc : s->eng->profile_stage(p, fmask, reps, ms4);
 }
+static int fft_plans_of(llg::EngineBase* eng, int32_t* rows, int32_t nr, int32_t* cols, int32_t nc) {
+    std::vector<int> r(std::max(nr, 0)), c(std::max(nc, 0));
+    for (auto& x : r) x = -2;
+    for (auto& x : c) x = -2;
+    eng->fft_plans(r.data(), nr, c.data(), nc);
+    for (int i = 0; i < nr; ++i) rows[i] = r[i];
+    for (int i = 0; i < nc; ++i) cols[i] = c[i];
+    return LLG_OK;
+}
+
+int llg_solver_fft_plans(llg_solver* s, int32_t* row_plan, int32_t* col_plan) {
+    int rc = bind(s);
+    if (!rc && (!row_plan || !col_plan)) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc : fft_plans_of(s->eng.get(), row_plan, 1, col_plan, 1);
+}
+
 int llg_solver_launch_count(llg_solver* s, int64_t* out) {
     int rc = bind(s);
     if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");
@@ -1865,6 +2017,12 @@ int llg_batch_compute_energy(llg_batch* b, const double* b_ext, llg_energy_break
     if (!rc && (!b_ext || !out)) rc = set_error(LLG_ERR_INVALID, "null argument");
     return rc ? rc : b->eng->energy(b_ext, out);
 }
+int llg_batch_fft_plans(llg_batch* b, int32_t* row_plans, int32_t n_row, int32_t* col_plans, int32_t n_col) {
+    int rc = bind(b);
+    if (!rc && ((n_row > 0 && !row_plans) || (n_col > 0 && !col_plans))) rc = set_error(LLG_ERR_INVALID, "null argument");
+    return rc ? rc : fft_plans_of(b->eng.get(), row_plans, n_row, col_plans, n_col);
+}
+
 int llg_batch_launch_count(llg_batch* b, int64_t* out) {
     int rc = bind(b);
     if (!rc && !out) rc = set_error(LLG_ERR_INVALID, "null argument");

@@ -95,8 +95,8 @@ struct FilmDev {
     const uint8_t* mask;
     const void* tw_row;           // exp(-2 pi i k / (2nx)), k < 2nx
     const void* tw_col;           // exp(-2 pi i k / (2ny)), k < 2ny
-    const void* twp_row;          // register-FFT pass tables for length nx (fast path)
-    const void* twp_col;          // register-FFT pass tables for length ny (fast path)
+    const void* twp_row[2];       // register-FFT pass tables for length nx, per radix plan (fast path)
+    const void* twp_col[2];       // register-FFT pass tables for length ny, per radix plan (fast path)
     double* red_part;             // [nblk][RED_NSLOT] per-block partial reductions
     StepState* st;
 };

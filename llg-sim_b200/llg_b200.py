@@ -191,6 +191,8 @@ def lib():
             "llg_demag_kernel_kspace": (C.c_int, [vp, dp]),
             "llg_profile_stage": (C.c_int, [vp, P(_Params), i32, i32, dp]),
             "llg_solver_launch_count": (C.c_int, [vp, P(i64)]),
+            "llg_solver_fft_plans": (C.c_int, [vp, P(i32), P(i32)]),
+            "llg_batch_fft_plans": (C.c_int, [vp, P(i32), i32, P(i32), i32]),
             "llg_demag_field_noalloc": (C.c_int, [i64, i64, C.c_double, vp, vp, vp, vp]),
             "llg_batch_create": (C.c_int, [vp, i32, P(_Grid), P(_Material), i32, P(C.c_void_p), P(vp)]),
             "llg_batch_destroy": (C.c_int, [vp]),
@@ -453,6 +455,12 @@ class Solver:
         out = np.empty(4)
         _check(lib().llg_profile_stage(self.h, C.byref(p), int(field_mask), int(reps), _dp(out)))
         return out
+
+    def fft_plans(self):
+        """(row plan, column plan) the autotuner chose: 0 default, 1 alternative, -1 generic kernels."""
+        r, c = C.c_int32(), C.c_int32()
+        _check(lib().llg_solver_fft_plans(self.h, C.byref(r), C.byref(c)))
+        return r.value, c.value
 
     def launch_count(self):
         out = C.c_int64()

@@ -1,23 +1,27 @@
-"""Train the learned warm-start network on relaxations computed by this library.
+"""Train the learned warm-start network on relaxations computed by this library,
+on the GPU, with this library's own tensor-core kernels.
 
-    python llg-sim_b200/warmstart_train.py --films 256 --out <dir>
+    python llg-sim_b200/warmstart_train.py --films 20000 --out <dir>
 
-1. Data: holey 128x128 films (workloads.holey_film_batch: 0-6 circular holes,
-   D U[0, 2e-3], 0-30 mT in-plane), random unit m0, relaxed on the GPU with the
-   batched device relax (FP32, max |m x B| below 1e-3 T; FP32 field round-off
-   puts a floor near 2e-4 T under the tightening stages).
-2. Training: the network of conv_tc.cu (six 3x3 convolutions, 32 channels, ReLU)
-   in PyTorch with BF16 autocast, loss = mean over film cells of 1 - cos(angle)
-   between the normalised output and the relaxed m.
+1. Data: holey 128x128 films (workloads.holey_film_batch: 0-6 circular holes of
+   radius 8-24 cells, D U[0, 2e-3], 0-30 mT in-plane), random unit m0 (zero in
+   the holes), relaxed on the GPU by the batched device relax (FP32, max |m x B|
+   below --torque; FP32 field round-off puts a floor near 2e-4 T under the
+   tightening stages).  The (m0, mask, B_ext) -> relaxed m pairs stay on the GPU.
+2. Training: WarmStartTrainer (train_tc.cu): forward and input-gradient
+   convolutions and the weight-gradient kernel on the tensor cores (BF16
+   operands, FP32 accumulation), loss = mean over film cells of 1 - cos(angle)
+   between the normalised output and the relaxed m, Adam on FP32 master weights
+   with a cosine learning-rate decay, minibatches drawn by a seeded permutation.
+   PyTorch only holds the device arrays (plumbing); no torch operator runs in
+   the training loop.
 3. Export: the flat FP32 parameter vector in the layout llg_warmstart_create
    takes (per layer W[cout][3][3][cin] then b[cout]) to <out>/warmstart.npy,
-   a training log and summary (and the dataset with --save-dataset).
-
-The tensor-core kernels run the exported network; PyTorch is used here only as
-the offline training tool.
+   a log and a summary (train / held-out loss per epoch, relax statistics).
 """
 import argparse
 import json
+import math
 import os
 import sys
 import time
@@ -32,120 +36,140 @@ import llg_b200 as L  # noqa: E402
 import workloads as W  # noqa: E402
 
 LAYERS = ((7, 32), (32, 32), (32, 32), (32, 32), (32, 32), (32, 3))
-FIELD_SCALE = 1.0 / 0.05
 
 
-def relax_dataset(n, size, seed, chunk, max_steps, log):
+def init_params(seed):
+    """He-normal weights, small biases, in the flat layout of llg_warmstart_create."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for ci, co in LAYERS:
+        out.append(rng.normal(0.0, math.sqrt(2.0 / (9 * ci)), size=(co, 3, 3, ci)).reshape(-1))
+        out.append(np.zeros(co))
+    return np.concatenate(out).astype(np.float32)
+
+
+def relax_dataset(n, size, seed, chunk, max_steps, torque, log):
+    """Relaxed films on the host: m0 and m_relaxed as FP32 SoA [n][3][size*size],
+    masks uint8 [n][size*size], B_ext [n][3], accepted steps [n]."""
     films, rx = W.holey_film_batch(n, size, seed=seed)
-    m0s, masks, bexts, mrel, steps = [], [], [], [], []
+    hw = size * size
+    m0 = np.empty((n, 3, hw), dtype=np.float32)
+    mrel = np.empty((n, 3, hw), dtype=np.float32)
+    masks = np.empty((n, hw), dtype=np.uint8)
+    bext = np.empty((n, 3))
+    steps = np.empty(n, dtype=np.int64)
     for c0 in range(0, n, chunk):
         part = films[c0:c0 + chunk]
         b = L.Batch([f.grid(L) for f in part], [f.material(L) for f in part], L.FP32, masks=[f.mask for f in part])
         for i, f in enumerate(part):
-            m = L.init_random(f.n, seed * 100000 + c0 + i)
+            m = L.init_random(f.n, seed * 1000003 + c0 + i)
             m[f.mask == 0] = 0.0
             b.set_state(i, m)
-            m0s.append(m)
-            masks.append(f.mask)
-            bexts.append(f.b_ext)
-        st = L.RelaxSettings.default(torque_threshold=1e-3, max_err=rx["max_err"], headroom=rx["headroom"],
+            m0[c0 + i] = m.T
+            masks[c0 + i] = f.mask
+            bext[c0 + i] = f.b_ext
+        st = L.RelaxSettings.default(torque_threshold=torque, max_err=rx["max_err"], headroom=rx["headroom"],
                                      dt_min=rx["dt_min"], dt_max=rx["dt_max"], max_accepted_steps=max_steps)
         P = [L.LLGParams(W.GAMMA, f.alpha, rx["dt0"], f.b_ext) for f in part]
         t0 = time.time()
         reps = b.relax(P, L.FULL, st)
         for i in range(len(part)):
-            mrel.append(b.get_state(i))
-            steps.append(reps[i].accepted_steps)
-        log(f"relaxed films {c0}..{c0 + len(part) - 1} in {time.time() - t0:.1f} s, steps "
-            f"{int(np.mean(steps[-len(part):]))} mean / {int(np.max(steps[-len(part):]))} max")
+            mrel[c0 + i] = b.get_state(i).T
+            steps[c0 + i] = reps[i].accepted_steps
+        s = steps[c0:c0 + len(part)]
+        log(f"relaxed films {c0}..{c0 + len(part) - 1} in {time.time() - t0:.1f} s, steps {int(s.mean())} mean / "
+            f"{int(s.max())} max, {int((s >= max_steps).sum())} at the cap")
         b.close()
-    return (np.stack(m0s), np.stack(masks), np.array(bexts), np.stack(mrel), np.array(steps))
+    return m0, masks, bext, mrel, steps
 
 
-def to_input(m0, mask, bext, size):
+def train(data, size, epochs, batch, lr, log, seed=0, holdout=0.02, params=None):
     import torch
 
+    m0, masks, bext, mrel, _ = data
     n = m0.shape[0]
-    inside = (mask != 0).astype(np.float32)
-    x = np.zeros((n, 7, size * size), dtype=np.float32)
-    x[:, 0:3] = (m0 * inside[..., None]).transpose(0, 2, 1)
-    x[:, 3] = inside
-    x[:, 4:7] = (bext.astype(np.float32) * np.float32(FIELD_SCALE))[..., None]
-    return torch.from_numpy(x.reshape(n, 7, size, size))
-
-
-def build_model():
-    import torch.nn as nn
-
-    mods = []
-    for li, (ci, co) in enumerate(LAYERS):
-        mods.append(nn.Conv2d(ci, co, 3, padding=1))
-        if li < len(LAYERS) - 1:
-            mods.append(nn.ReLU())
-    return nn.Sequential(*mods)
-
-
-def export_params(model):
-    import torch.nn as nn
-
-    out = []
-    for mod in model:
-        if isinstance(mod, nn.Conv2d):
-            w = mod.weight.detach().float().cpu().numpy()          # [cout][cin][3][3]
-            out.append(w.transpose(0, 2, 3, 1).reshape(-1))        # -> [cout][3][3][cin]
-            out.append(mod.bias.detach().float().cpu().numpy())
-    return np.concatenate(out).astype(np.float32)
-
-
-def train(data, size, epochs, batch, lr, log, seed=0):
-    import torch
-
-    torch.manual_seed(seed)
-    m0, mask, bext, mrel, _ = data
-    x = to_input(m0, mask, bext, size)
-    y = torch.from_numpy(mrel.astype(np.float32).transpose(0, 2, 1).reshape(-1, 3, size, size))
-    w = torch.from_numpy((mask != 0).astype(np.float32).reshape(-1, 1, size, size))
     dev = "cuda"
-    x, y, w = x.to(dev), y.to(dev), w.to(dev)
-    model = build_model().to(dev)
-    opt = torch.optim.Adam(model.parameters(), lr=lr)
-    n = x.shape[0]
-    steps = epochs * ((n + batch - 1) // batch)
-    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, steps)
+    d_m0 = torch.from_numpy(m0).to(dev)
+    d_t = torch.from_numpy(mrel).to(dev)
+    d_k = torch.from_numpy(masks).to(dev)
+    d_b = torch.from_numpy(np.ascontiguousarray(bext, dtype=np.float64)).to(dev)
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(n)
+    n_hold = max(1, int(round(holdout * n))) if n > 8 else 0
+    hold, train_idx = order[:n_hold], order[n_hold:]
+    hw = size * size
+    p0 = init_params(seed + 1) if params is None else params
+    tr = L.WarmStartTrainer(p0, batch * hw)
+    # minibatch buffers (gathered on the device by index)
+    bm0 = torch.empty((batch, 3, hw), dtype=torch.float32, device=dev)
+    bt = torch.empty_like(bm0)
+    bk = torch.empty((batch, hw), dtype=torch.uint8, device=dev)
+    bb = torch.empty((batch, 3), dtype=torch.float64, device=dev)
+
+    def gather(idx):
+        ii = torch.from_numpy(np.asarray(idx, dtype=np.int64)).to(dev)
+        k = len(idx)
+        torch.index_select(d_m0, 0, ii, out=bm0[:k])
+        torch.index_select(d_t, 0, ii, out=bt[:k])
+        torch.index_select(d_k, 0, ii, out=bk[:k])
+        torch.index_select(d_b, 0, ii, out=bb[:k])
+        return k, (bm0.data_ptr(), bk.data_ptr(), bb.data_ptr(), bt.data_ptr())
+
+    def held_out_loss():
+        if n_hold == 0:
+            return None
+        tot = cells = 0.0
+        for b0 in range(0, n_hold, batch):
+            idx = hold[b0:b0 + batch]
+            k, ptrs = gather(idx)
+            loss, _ = tr.gradients(k, size, size, *ptrs)
+            c = float(masks[idx].astype(bool).sum())
+            tot += loss * c
+            cells += c
+        return tot / max(cells, 1.0)
+
+    steps_per_epoch = (len(train_idx) + batch - 1) // batch
+    total = epochs * steps_per_epoch
     hist = []
+    step = 0
+    t0 = time.time()
     for ep in range(epochs):
-        perm = torch.randperm(n, device=dev)
+        perm = rng.permutation(train_idx)
         tot = 0.0
-        for b0 in range(0, n, batch):
+        cnt = 0
+        for b0 in range(0, len(perm), batch):
             idx = perm[b0:b0 + batch]
-            with torch.autocast("cuda", dtype=torch.bfloat16):
-                out = model(x[idx])
-            out = out.float()
-            out = out / (out.norm(dim=1, keepdim=True) + 1e-12)
-            cos = (out * y[idx]).sum(dim=1, keepdim=True)
-            loss = ((1.0 - cos) * w[idx]).sum() / w[idx].sum().clamp(min=1.0)
-            opt.zero_grad(set_to_none=True)
-            loss.backward()
-            opt.step()
-            sched.step()
-            tot += float(loss) * len(idx)
-        hist.append(tot / n)
-        log(f"epoch {ep}: loss {hist[-1]:.5f}")
-    return model, hist
+            k, ptrs = gather(idx)
+            cur = lr * 0.5 * (1.0 + math.cos(math.pi * step / max(total, 1)))
+            read = (b0 // batch) % 25 == 0
+            loss = tr.step(k, size, size, *ptrs, lr=cur, read_loss=read)
+            if read:
+                tot += loss
+                cnt += 1
+            step += 1
+        tr.sync()
+        hl = held_out_loss()
+        hist.append({"epoch": ep, "train_loss": tot / max(cnt, 1), "held_out_loss": hl,
+                     "seconds": time.time() - t0})
+        log(f"epoch {ep}: train loss {hist[-1]['train_loss']:.5f}, held-out loss {hl}, {time.time() - t0:.1f} s")
+    params = tr.params()
+    tr.close()
+    return params, hist, {"train_films": int(len(train_idx)), "held_out_films": int(n_hold), "steps": step}
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--films", type=int, default=256)
+    ap.add_argument("--films", type=int, default=20000)
     ap.add_argument("--size", type=int, default=128)
-    ap.add_argument("--chunk", type=int, default=128)
-    ap.add_argument("--max-steps", type=int, default=40000)
-    ap.add_argument("--epochs", type=int, default=60)
-    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--chunk", type=int, default=2048)
+    ap.add_argument("--max-steps", type=int, default=30000)
+    ap.add_argument("--torque", type=float, default=1e-3)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=21)
+    ap.add_argument("--init", default=None, help="start from these parameters (.npy) instead of a fresh draw")
     ap.add_argument("--out", required=True)
-    ap.add_argument("--save-dataset", action="store_true")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     logf = open(os.path.join(args.out, "train_log.txt"), "w")
@@ -156,20 +180,23 @@ def main():
         logf.flush()
 
     t0 = time.time()
-    data = relax_dataset(args.films, args.size, args.seed, args.chunk, args.max_steps, log)
-    if args.save_dataset:
-        np.savez_compressed(os.path.join(args.out, "dataset.npz"), m0=data[0].astype(np.float32), mask=data[1],
-                            bext=data[2], m_relaxed=data[3].astype(np.float32), steps=data[4])
-    log(f"dataset: {args.films} films in {time.time() - t0:.1f} s")
+    data = relax_dataset(args.films, args.size, args.seed, args.chunk, args.max_steps, args.torque, log)
+    t_data = time.time() - t0
+    log(f"dataset: {args.films} films in {t_data:.1f} s")
+    init = np.load(args.init) if args.init else None
     t1 = time.time()
-    model, hist = train(data, args.size, args.epochs, args.batch, args.lr, log)
-    params = export_params(model)
+    params, hist, info = train(data, args.size, args.epochs, args.batch, args.lr, log, seed=args.seed, params=init)
     assert params.size == L.WarmStartNet.param_count()
     np.save(os.path.join(args.out, "warmstart.npy"), params)
-    log(f"training: {time.time() - t1:.1f} s, final loss {hist[-1]:.5f}")
-    json.dump({"films": args.films, "size": args.size, "epochs": args.epochs, "loss": hist,
-               "relax_steps_mean": float(np.mean(data[4])), "seconds": time.time() - t0},
-              open(os.path.join(args.out, "train_summary.json"), "w"))
+    log(f"training: {time.time() - t1:.1f} s, final train loss {hist[-1]['train_loss']:.5f}")
+    steps = data[4]
+    json.dump({"films": args.films, "size": args.size, "epochs": args.epochs, "batch": args.batch, "lr": args.lr,
+               "torque_threshold": args.torque, "max_steps": args.max_steps, "history": hist, **info,
+               "relax_steps_mean": float(steps.mean()), "relax_steps_max": int(steps.max()),
+               "relax_at_cap": int((steps >= args.max_steps).sum()), "dataset_seconds": t_data,
+               "training_seconds": time.time() - t1, "trainer": "llg_wstrain (tcgen05 forward / input-gradient / "
+                                                                 "weight-gradient kernels, Adam on the device)"},
+              open(os.path.join(args.out, "train_summary.json"), "w"), indent=1)
 
 
 if __name__ == "__main__":

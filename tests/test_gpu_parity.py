@@ -222,3 +222,33 @@ def test_register_fft_matches_generic_kernels(orc, gpu, nx, ny, monkeypatch):
         assert rf[1] == rg[1]
         p.dt = rf[2]
     assert np.abs(fast.get_state() - gen.get_state()).max() <= 1e-12
+
+
+PLAN1_SHAPES = [(1024, 128, 0), (2048, 256, 0), (64, 1024, 0), (512, 256, 1), (128, 512, 1)]
+
+
+@pytest.mark.parametrize("nx,ny,prec", PLAN1_SHAPES)
+def test_fft_plan1_matches_oracle(orc, gpu, monkeypatch, nx, ny, prec):
+    """The alternative register-FFT radix plans (half the registers per thread),
+    forced with LLG_B200_FFT_PLAN=1, against the oracle: fields and three RK45 steps."""
+    monkeypatch.setenv("LLG_B200_FFT_PLAN", "1")
+    c = case(nx, ny, dmi=2e-3, k_u=1e5)
+    g = gpu_solver(gpu, c, prec)
+    monkeypatch.delenv("LLG_B200_FFT_PLAN")
+    rp, cp = g.fft_plans()
+    assert cp == 1 and rp in (0, 1)
+    o = oracle_solver(orc, c)
+    m = random_m(orc, nx * ny, 13 + nx)
+    g.set_state(m)
+    bext = (0.01, 0.0, -0.02)
+    p = gpu.LLGParams(GAMMA, 0.1, 1e-13, bext)
+    assert rel_err(g.build_h_eff(p, 2), o.build_h_eff(m, bext, 2)) <= TOL[prec]
+    assert rel_err(g.compute_demag_field(), o.demag_field(m)) <= TOL[prec]
+    po = orc.make_params(GAMMA, 0.1, 1e-13, bext)
+    mo = m.copy()
+    for _ in range(3):
+        ro = o.step_rk45(mo, po, 2, 1e-5, 0.8, 1e-19, 1e-11)
+        rg = g.step_rk45(p, 2, 1e-5, 0.8, 1e-19, 1e-11)
+        assert ro[1] == rg[1]
+        p.dt = po.dt
+    assert np.abs(g.get_state() - mo).max() <= (1e-12 if prec else 2e-6)
