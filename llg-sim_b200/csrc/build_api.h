@@ -1,6 +1,7 @@
 // build_api.h — host-side entry points shared between the compilation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <vector>
 #include "../../include/llg_b200.h"
 #include "types.cuh"
 
@@ -10,6 +11,8 @@ void llg_set_error_message(const char* msg);
 namespace llg {
 
 FftPlan make_plan(int L);
+// Alternative radix plans of length L for the autotuner (the first is make_plan(L)).
+std::vector<FftPlan> plan_candidates(int L);
 cudaError_t launch_twiddles(void* tw, int L2, bool fp64, cudaStream_t s);
 template <typename R>
 cudaError_t launch_fft_strided(void* data, int L, const void* tw2, long long elem_stride, int nsig_a,

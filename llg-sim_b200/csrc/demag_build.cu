@@ -13,6 +13,9 @@
 //      1/(px*py) and cast to the solver precision.
 // Each integration sample differences two charge/(4 pi r^3) pole terms that
 // cancel at large r, so all of this stays FP64.
+#include <algorithm>
+#include <vector>
+
 #include "build_api.h"
 #include "fft_smem.cuh"
 #include "field_kernels.cuh"
@@ -244,6 +247,58 @@ FftPlan make_plan(int L) {
         }
     }
     return p;
+}
+
+// Candidate radix plans of the generic Stockham transform of length L (any radix
+// order is a valid Stockham plan): the powers of two grouped mostly as 8s or
+// mostly as 4s, each with the odd factors last (make_plan's order), first, or the
+// powers of two in ascending order.  The first candidate is make_plan(L).
+std::vector<FftPlan> plan_candidates(int L) {
+    std::vector<FftPlan> out;
+    out.push_back(make_plan(L));
+    int r = L, e2 = 0;
+    while (r % 2 == 0 && r > 1) {
+        r /= 2;
+        ++e2;
+    }
+    std::vector<int> odd;
+    for (int f : {3, 5}) while (r % f == 0) { odd.push_back(f); r /= f; }
+    for (int f = 7; r > 1; f += 2) while (r % f == 0) { odd.push_back(f); r /= f; }
+    auto twos = [&](bool eights) {
+        std::vector<int> v;
+        int e = e2;
+        if (eights) {
+            while (e >= 3) { v.push_back(8); e -= 3; }
+            if (e == 2) v.push_back(4);
+            if (e == 1) v.push_back(2);
+        } else {
+            while (e >= 2) { v.push_back(4); e -= 2; }
+            if (e == 1) v.push_back(2);
+        }
+        return v;
+    };
+    auto add = [&](const std::vector<int>& rad) {
+        if (rad.empty() || (int)rad.size() > kMaxRadices) return;
+        FftPlan p{};
+        p.L = L;
+        p.npass = (int)rad.size();
+        for (size_t i = 0; i < rad.size(); ++i) p.radix[i] = rad[i];
+        for (const FftPlan& q : out)
+            if (q.npass == p.npass && std::equal(q.radix, q.radix + q.npass, p.radix)) return;
+        out.push_back(p);
+    };
+    for (bool eights : {true, false}) {
+        std::vector<int> t = twos(eights);
+        std::vector<int> a = t, b = odd, c = t;
+        a.insert(a.end(), odd.begin(), odd.end());           // powers of two first
+        b.insert(b.end(), t.begin(), t.end());               // odd factors first
+        std::reverse(c.begin(), c.end());                    // ascending powers of two, then odd
+        c.insert(c.end(), odd.begin(), odd.end());
+        add(a);
+        add(b);
+        add(c);
+    }
+    return out;
 }
 
 cudaError_t launch_twiddles(void* tw, int L2, bool fp64, cudaStream_t s) {

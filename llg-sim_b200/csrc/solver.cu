@@ -362,6 +362,7 @@ struct Engine final : EngineBase {
     std::vector<std::array<LaunchGeom, 2>> rseg_alt, cseg_alt;
     std::vector<std::array<char, 2>> rseg_has, cseg_has;
     std::vector<std::array<std::array<int, 4>, 2>> rocc;
+    std::vector<std::vector<int>> rseg_films, cseg_films;   // films of each segment
     std::vector<std::array<int, 2>> cocc;
 
     int nfilms() const override { return nf; }
@@ -647,6 +648,13 @@ struct Engine final : EngineBase {
                     has[v] = 1;
                     occ[v] = {fb, ib, ub, zb};
                 }
+                {
+                    std::vector<int> fl;
+                    for (size_t q = 0; q < sp.second.second; ++q) fl.push_back(rows[sp.second.first + q].film);
+                    std::sort(fl.begin(), fl.end());
+                    fl.erase(std::unique(fl.begin(), fl.end()), fl.end());
+                    rseg_films.push_back(fl);
+                }
                 rseg.push_back(alt[0]);
                 rseg_alt.push_back(alt);
                 rseg_has.push_back(has);
@@ -658,6 +666,11 @@ struct Engine final : EngineBase {
                 const int L = sp.first ? sp.first / 2 : 0, v = sp.first ? sp.first % 2 : 0;
                 if (!col_index.count(L)) {
                     col_index[L] = cseg.size();
+                    std::vector<int> fl;
+                    for (size_t q = 0; q < sp.second.second; ++q) fl.push_back(cols[sp.second.first + q].film);
+                    std::sort(fl.begin(), fl.end());
+                    fl.erase(std::unique(fl.begin(), fl.end()), fl.end());
+                    cseg_films.push_back(fl);
                     cseg.push_back(LaunchGeom{});
                     cseg_alt.push_back({});
                     cseg_has.push_back({0, 0});
@@ -825,9 +838,83 @@ struct Engine final : EngineBase {
             if (tuning && (rc = time_col(v, &t))) return rc;
             cseg[i] = cseg_alt[i][v];
         }
+        // generic shared-memory kernels: the radix order / grouping of each length,
+        // timed on the segment's passes at its current grid
+        auto time_pass = [&](int kind, LaunchGeom& g, float* t) -> int {
+            const int whiches[2][2] = {{0, 2}, {1, 1}};
+            const int nw = kind == 0 ? 2 : 1;
+            for (int w = 0; w < 2; ++w)
+                for (int q = 0; q < nw; ++q) CUDA_TRY(launch_one<R>(whiches[kind][q], stage, g, stream));
+            CUDA_TRY(cudaEventRecord(e0, stream));
+            for (int r = 0; r < 4; ++r)
+                for (int q = 0; q < nw; ++q) CUDA_TRY(launch_one<R>(whiches[kind][q], stage, g, stream));
+            CUDA_TRY(cudaEventRecord(e1, stream));
+            CUDA_TRY(cudaEventSynchronize(e1));
+            CUDA_TRY(cudaEventElapsedTime(t, e0, e1));
+            return LLG_OK;
+        };
+        if ((rc = tune_generic_plans(forced, tuning, time_pass))) return rc;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         invalidate_fsal_host();
+        return LLG_OK;
+    }
+
+    // Radix plans of the generic shared-memory transforms: for every length that a
+    // generic row or column segment transforms, the candidate orders / groupings of
+    // its radices (plan_candidates) are timed on that segment's pass, one length at a
+    // time with the others fixed, and the fastest is kept for every film of that
+    // length.  Like the register-FFT plans, the first decision per (precision, pass,
+    // length) holds for the whole process.
+    template <typename TimeFn>
+    int tune_generic_plans(int forced, bool tuning, TimeFn&& time_pass) {
+        for (int kind = 0; kind < 2; ++kind) {
+            auto& segs = kind == 0 ? rseg : cseg;
+            auto& films = kind == 0 ? rseg_films : cseg_films;
+            for (size_t i = 0; i < segs.size(); ++i) {
+                LaunchGeom& sg = segs[i];
+                if ((kind == 0 ? sg.fast_row : sg.fast_col) != 0) continue;
+                std::vector<int> lengths;
+                for (int f : films[i]) lengths.push_back(kind == 0 ? fh[f].nx : fh[f].ny);
+                std::sort(lengths.begin(), lengths.end());
+                lengths.erase(std::unique(lengths.begin(), lengths.end()), lengths.end());
+                for (int L : lengths) {
+                    const std::vector<FftPlan> cand = plan_candidates(L);
+                    auto apply = [&](const FftPlan& pl) {
+                        for (int f : films[i]) {
+                            if ((kind == 0 ? fh[f].nx : fh[f].ny) != L) continue;
+                            (kind == 0 ? fh[f].plan_row : fh[f].plan_col) = pl;
+                        }
+                        return upload_films();
+                    };
+                    const std::tuple<int, int, int> key{(int)sizeof(R), 2 + kind, L};
+                    int chosen = -1;
+                    {
+                        std::lock_guard<std::mutex> lock(g_plan_mutex);
+                        auto it = g_plan_cache.find(key);
+                        if (it != g_plan_cache.end()) chosen = it->second;
+                    }
+                    if (chosen < 0 && tuning && forced < 0 && cand.size() > 1) {
+                        float best = 1e30f;
+                        for (size_t c = 0; c < cand.size(); ++c) {
+                            int rc;
+                            if ((rc = apply(cand[c]))) return rc;
+                            float t = 0.f;
+                            if ((rc = time_pass(kind, sg, &t))) return rc;
+                            if (t < best) {
+                                best = t;
+                                chosen = (int)c;
+                            }
+                        }
+                        std::lock_guard<std::mutex> lock(g_plan_mutex);
+                        g_plan_cache.emplace(key, chosen);
+                    }
+                    if (chosen < 0 || chosen >= (int)cand.size()) chosen = 0;
+                    int rc;
+                    if ((rc = apply(cand[chosen]))) return rc;
+                }
+            }
+        }
         return LLG_OK;
     }
 
