@@ -48,9 +48,10 @@ def init_params(seed):
     return np.concatenate(out).astype(np.float32)
 
 
-def relax_dataset(n, size, seed, chunk, max_steps, torque, log):
+def relax_dataset(n, size, seed, chunk, max_steps, torque, log, budget_s=None):
     """Relaxed films on the host: m0 and m_relaxed as FP32 SoA [n][3][size*size],
-    masks uint8 [n][size*size], B_ext [n][3], accepted steps [n]."""
+    masks uint8 [n][size*size], B_ext [n][3], accepted steps [n].  With budget_s, no
+    new chunk starts after that many seconds (the films done so far are returned)."""
     films, rx = W.holey_film_batch(n, size, seed=seed)
     hw = size * size
     m0 = np.empty((n, 3, hw), dtype=np.float32)
@@ -58,7 +59,12 @@ def relax_dataset(n, size, seed, chunk, max_steps, torque, log):
     masks = np.empty((n, hw), dtype=np.uint8)
     bext = np.empty((n, 3))
     steps = np.empty(n, dtype=np.int64)
+    t_start = time.time()
+    done = 0
     for c0 in range(0, n, chunk):
+        if budget_s is not None and time.time() - t_start > budget_s:
+            log(f"dataset budget of {budget_s:.0f} s reached after {done} films")
+            break
         part = films[c0:c0 + chunk]
         b = L.Batch([f.grid(L) for f in part], [f.material(L) for f in part], L.FP32, masks=[f.mask for f in part])
         for i, f in enumerate(part):
@@ -80,7 +86,8 @@ def relax_dataset(n, size, seed, chunk, max_steps, torque, log):
         log(f"relaxed films {c0}..{c0 + len(part) - 1} in {time.time() - t0:.1f} s, steps {int(s.mean())} mean / "
             f"{int(s.max())} max, {int((s >= max_steps).sum())} at the cap")
         b.close()
-    return m0, masks, bext, mrel, steps
+        done = c0 + len(part)
+    return m0[:done], masks[:done], bext[:done], mrel[:done], steps[:done]
 
 
 def train(data, size, epochs, batch, lr, log, seed=0, holdout=0.02, params=None):
@@ -169,6 +176,8 @@ def main():
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=21)
     ap.add_argument("--init", default=None, help="start from these parameters (.npy) instead of a fresh draw")
+    ap.add_argument("--data-budget", type=float, default=None, help="seconds after which no new relax chunk starts")
+    ap.add_argument("--drop-capped", action="store_true", help="train only on films that reached the torque")
     ap.add_argument("--out", required=True)
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
@@ -180,17 +189,24 @@ def main():
         logf.flush()
 
     t0 = time.time()
-    data = relax_dataset(args.films, args.size, args.seed, args.chunk, args.max_steps, args.torque, log)
+    data = relax_dataset(args.films, args.size, args.seed, args.chunk, args.max_steps, args.torque, log,
+                         args.data_budget)
     t_data = time.time() - t0
-    log(f"dataset: {args.films} films in {t_data:.1f} s")
+    n_rel = len(data[4])
+    log(f"dataset: {n_rel} films relaxed in {t_data:.1f} s")
+    steps_all = data[4]
+    if args.drop_capped:
+        keep = steps_all < args.max_steps
+        data = tuple(x[keep] for x in data)
+        log(f"training on {int(keep.sum())} films that reached the torque ({int((~keep).sum())} at the cap dropped)")
     init = np.load(args.init) if args.init else None
     t1 = time.time()
     params, hist, info = train(data, args.size, args.epochs, args.batch, args.lr, log, seed=args.seed, params=init)
     assert params.size == L.WarmStartNet.param_count()
     np.save(os.path.join(args.out, "warmstart.npy"), params)
     log(f"training: {time.time() - t1:.1f} s, final train loss {hist[-1]['train_loss']:.5f}")
-    steps = data[4]
-    json.dump({"films": args.films, "size": args.size, "epochs": args.epochs, "batch": args.batch, "lr": args.lr,
+    steps = steps_all
+    json.dump({"films_requested": args.films, "films": n_rel, "films_trained": int(len(data[4])), "size": args.size, "epochs": args.epochs, "batch": args.batch, "lr": args.lr,
                "torque_threshold": args.torque, "max_steps": args.max_steps, "history": hist, **info,
                "relax_steps_mean": float(steps.mean()), "relax_steps_max": int(steps.max()),
                "relax_at_cap": int((steps >= args.max_steps).sum()), "dataset_seconds": t_data,
