@@ -259,10 +259,13 @@ int llg_batch_launch_count(llg_batch* b, int64_t* out);
  * pass that ends this stage and starts the next (0 when no film uses it).
  * llg_solver_launch_count: kernels this solver has issued so far. */
 int llg_profile_stage(llg_solver* s, const llg_params* params, int32_t field_mask, int32_t reps, double* ms4);
-/* Register-FFT radix plan the autotuner chose for the row and the column pass
- * (0 default, 1 alternative with half the registers per thread; -1 where the
- * pass runs the generic shared-memory kernels).  For a batch, one entry per
- * launch segment (films grouped by length), in segment order; unused entries -2. */
+/* Register-FFT form the autotuner chose for the row and the column pass.  Row:
+ * the radix plan (0 default, 1 alternative with half the registers per thread).
+ * Column: 2 * plan + lean, lean = 1 when the pass reads its twiddle tables and
+ * kernel columns through L1 instead of staging them in shared memory (more
+ * resident blocks).  -1 where the pass runs the generic shared-memory kernels.
+ * For a batch, one entry per launch segment (films grouped by length), in
+ * segment order; unused entries -2. */
 int llg_solver_fft_plans(llg_solver* s, int32_t* row_plan, int32_t* col_plan);
 int llg_batch_fft_plans(llg_batch* b, int32_t* row_plans, int32_t n_row, int32_t* col_plans, int32_t n_col);
 int llg_solver_launch_count(llg_solver* s, int64_t* out);

@@ -54,7 +54,7 @@ struct LaunchGeom {
     bool any_demag;
     bool fuse_rows;   // end a stage and start the next in one row pass where possible
     int row_var;      // register-FFT radix plan of the row kernels (FPlan V)
-    int col_var;      // register-FFT radix plan of the column kernel (FPlan V)
+    int col_var;      // column kernel form: 2 * register-FFT radix plan (FPlan V) + lean form (0 / 1)
     int fast_row;     // register-FFT row kernels for L = nx (0: generic kernels)
     int fast_col;     // register-FFT column kernel for L = ny (0: generic kernel)
     int row_threads;

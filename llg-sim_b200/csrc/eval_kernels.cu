@@ -132,8 +132,10 @@ cudaError_t prepare_eval_kernels(size_t smem_row, size_t smem_col) {
             both((const void*)k_row_inverse_fast<R, L, 2, V>, sm);
             both((const void*)k_row_fused<R, L, V>, sm);
         }
-        if constexpr (ColCfg<R, L, V>::SMEM + kStaticSmemCol <= kSmemMax)
-            both((const void*)k_column_fast<R, L, V>, (int)ColCfg<R, L, V>::SMEM);
+        if constexpr (ColCfg<R, L, V>::SMEM + kStaticSmemCol <= kSmemMax) {
+            both((const void*)k_column_fast<R, L, V, false>, (int)ColCfg<R, L, V, false>::SMEM);
+            both((const void*)k_column_fast<R, L, V, true>, (int)ColCfg<R, L, V, true>::SMEM);
+        }
     };
     for (int L : {16, 32, 64, 128, 256, 512, 1024, 2048})
         for (int v = 0; v < 2; ++v) dispatch_LV<R>(L, v, set_all);
@@ -191,11 +193,19 @@ cudaError_t launch_one(int which, const EvalSpec& spec, const LaunchGeom& g, cud
         }
     } else {
         if (g.fast_col) {
-            dispatch_LV<R>(g.fast_col, g.col_var, [&](auto LC, auto VC) {
+            // col_var = 2 * radix plan + lean form
+            dispatch_LV<R>(g.fast_col, g.col_var / 2, [&](auto LC, auto VC) {
                 constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
-                if constexpr (ColCfg<R, L, V>::SMEM + kStaticSmemCol <= kSmemMax)
-                    k_column_fast<R, L, V><<<g.grid_col, ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::SMEM, s>>>(
-                        g.films, g.col_items, g.n_col_items, spec);
+                if constexpr (ColCfg<R, L, V>::SMEM + kStaticSmemCol <= kSmemMax) {
+                    if (g.col_var % 2)
+                        k_column_fast<R, L, V, true><<<g.grid_col, ColCfg<R, L, V, true>::THREADS,
+                                                       ColCfg<R, L, V, true>::SMEM, s>>>(g.films, g.col_items,
+                                                                                         g.n_col_items, spec);
+                    else
+                        k_column_fast<R, L, V, false><<<g.grid_col, ColCfg<R, L, V, false>::THREADS,
+                                                        ColCfg<R, L, V, false>::SMEM, s>>>(g.films, g.col_items,
+                                                                                           g.n_col_items, spec);
+                }
             });
         } else {
             k_column<R><<<g.grid_col, 256, g.smem_col, s>>>(g.films, g.col_items, g.n_col_items, spec);
@@ -256,12 +266,18 @@ void fast_occupancy(int nx, int ny, int row_var, int col_var, int* fwd_blocks_pe
             *fused_blocks_per_sm = std::max(1, d);
         }
     });
-    dispatch_LV<R>(ny, col_var, [&](auto LC, auto VC) {
+    dispatch_LV<R>(ny, col_var / 2, [&](auto LC, auto VC) {
         constexpr int L = decltype(LC)::value, V = decltype(VC)::value;
         if constexpr (ColCfg<R, L, V>::SMEM + kStaticSmemCol <= kSmemMax) {
             int a = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L, V>, ColCfg<R, L, V>::THREADS,
-                                                          ColCfg<R, L, V>::SMEM);
+            if (col_var % 2)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L, V, true>,
+                                                              ColCfg<R, L, V, true>::THREADS,
+                                                              ColCfg<R, L, V, true>::SMEM);
+            else
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_column_fast<R, L, V, false>,
+                                                              ColCfg<R, L, V, false>::THREADS,
+                                                              ColCfg<R, L, V, false>::SMEM);
             *col_blocks_per_sm = std::max(1, a);
         }
     });

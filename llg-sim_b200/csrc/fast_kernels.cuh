@@ -36,8 +36,11 @@ struct RowCfg {
 // even / odd ky bins).  Shared memory: the signal exchange buffers, the pass
 // tables and pre-twiddles, and the staging areas that the bulk copies of the
 // next item's spectrum columns (Xst, [3][NC][L]) and folded kernel columns
-// (Kst, [NC][L+1]) land in while the current item is transformed.
-template <typename R, int L, int V = 0>
+// (Kst, [NC][L+1]) land in while the current item is transformed.  The LEAN form
+// reads the tables and the kernel columns from global memory (through L1) and
+// keeps only the signal buffers and Xst in shared memory, so that more blocks fit
+// per SM.
+template <typename R, int L, int V = 0, bool LEAN = false>
 struct ColCfg {
     using P = FPlan<R, L, V>;
     static constexpr int G = P::G, E = P::E;
@@ -47,10 +50,10 @@ struct ColCfg {
     static constexpr int BUF = Pad<R, L, V>::size;
     static constexpr size_t al16(size_t b) { return (b + 15) / 16 * 16; }
     static constexpr size_t OFF_TW = al16(sizeof(cx<R>) * (size_t)NSIG * BUF);
-    static constexpr size_t OFF_PRE = al16(OFF_TW + sizeof(cx<R>) * (size_t)TwTab<R, L, V>::size);
-    static constexpr size_t OFF_XST = al16(OFF_PRE + sizeof(cx<R>) * (size_t)L);
+    static constexpr size_t OFF_PRE = al16(OFF_TW + (LEAN ? 0 : sizeof(cx<R>) * (size_t)TwTab<R, L, V>::size));
+    static constexpr size_t OFF_XST = al16(OFF_PRE + (LEAN ? 0 : sizeof(cx<R>) * (size_t)L));
     static constexpr size_t OFF_KST = al16(OFF_XST + sizeof(cx<R>) * 3 * (size_t)NC * L);
-    static constexpr size_t SMEM = al16(OFF_KST + sizeof(r4<R>) * (size_t)NC * (L + 1));
+    static constexpr size_t SMEM = al16(OFF_KST + (LEAN ? 0 : sizeof(r4<R>) * (size_t)NC * (L + 1)));
     static constexpr int MINB = V == 1 ? 2 : 1;   // plan 1: registers capped for two resident blocks
 };
 
@@ -264,11 +267,10 @@ __device__ __forceinline__ void col_issue_k(const FilmDev* __restrict__ films, c
     bulk_copy_g2s(kst, reinterpret_cast<const r4<R>*>(F.Khat) + (size_t)kx0 * (L + 1), bytes, bar);
 }
 
-template <typename R, int L, int V>
-__global__ void __launch_bounds__(ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::MINB) k_column_fast(const FilmDev* __restrict__ films,
-                                                                       const WorkItem* __restrict__ items, int nitems,
-                                                                       EvalSpec spec) {
-    using C = ColCfg<R, L, V>;
+template <typename R, int L, int V, bool LEAN>
+__global__ void __launch_bounds__(ColCfg<R, L, V, LEAN>::THREADS, ColCfg<R, L, V, LEAN>::MINB) k_column_fast(
+    const FilmDev* __restrict__ films, const WorkItem* __restrict__ items, int nitems, EvalSpec spec) {
+    using C = ColCfg<R, L, V, LEAN>;
     using FF = GroupFFT<R, L, false, V>;
     using FI = GroupFFT<R, L, true, V>;
     constexpr int G = C::G, E = C::E, BUF = C::BUF, NC = C::NC;
@@ -277,8 +279,8 @@ __global__ void __launch_bounds__(ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::MIN
     __shared__ uint64_t bars[2];   // 0: spectrum columns, 1: kernel columns
     __shared__ int s_timeout;
     cx<R>* buf = reinterpret_cast<cx<R>*>(smem_raw);
-    cx<R>* twp = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_TW);
-    cx<R>* pre = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_PRE);
+    const cx<R>* twp = reinterpret_cast<const cx<R>*>(smem_raw + C::OFF_TW);
+    const cx<R>* pre = reinterpret_cast<const cx<R>*>(smem_raw + C::OFF_PRE);
     cx<R>* xst = reinterpret_cast<cx<R>*>(smem_raw + C::OFF_XST);
     r4<R>* kst = reinterpret_cast<r4<R>*>(smem_raw + C::OFF_KST);
     const int tid = threadIdx.x, s = tid / G, t = tid % G;
@@ -293,7 +295,7 @@ __global__ void __launch_bounds__(ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::MIN
     const int it0 = blockIdx.x;
     if (tid == 0 && col_item_has<R, L>(films, items, nitems, spec, it0)) {
         col_issue_x<R, L, V>(films, items, it0, xst, &bars[0]);
-        col_issue_k<R, L, V>(films, items, it0, kst, &bars[1]);
+        if (!LEAN) col_issue_k<R, L, V>(films, items, it0, kst, &bars[1]);
     }
     uint32_t phase = 0;
     bool tables = false;
@@ -305,19 +307,22 @@ __global__ void __launch_bounds__(ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::MIN
             if (tid == 0 && has_next) {
                 fence_async_smem();
                 col_issue_x<R, L, V>(films, items, nxt, xst, &bars[0]);
-                col_issue_k<R, L, V>(films, items, nxt, kst, &bars[1]);
+                if (!LEAN) col_issue_k<R, L, V>(films, items, nxt, kst, &bars[1]);
             }
             continue;
         }
         const WorkItem w = items[it];
         const FilmDev& F = films[w.film];
-        if (!tables) {
-            load_tables<R>(twp, reinterpret_cast<const cx<R>*>(F.twp_col[V]), TwTab<R, L, V>::size, pre,
-                           reinterpret_cast<const cx<R>*>(F.tw_col), L);
+        if constexpr (LEAN) {
+            twp = reinterpret_cast<const cx<R>*>(F.twp_col[V]);
+            pre = reinterpret_cast<const cx<R>*>(F.tw_col);
+        } else if (!tables) {
+            load_tables<R>(const_cast<cx<R>*>(twp), reinterpret_cast<const cx<R>*>(F.twp_col[V]), TwTab<R, L, V>::size,
+                           const_cast<cx<R>*>(pre), reinterpret_cast<const cx<R>*>(F.tw_col), L);
             tables = true;
         }
         const bool okx = mbar_wait(&bars[0], phase);
-        const bool okk = mbar_wait(&bars[1], phase);
+        const bool okk = LEAN ? true : mbar_wait(&bars[1], phase);
         if (!(okx && okk)) s_timeout = 1;
         phase ^= 1u;
         __syncthreads();   // tables, staged columns, timeout flag
@@ -350,7 +355,8 @@ __global__ void __launch_bounds__(ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::MIN
 #pragma unroll
             for (int i = 0; i < E; ++i) buf[s * BUF + padi<E>(FF::out_index(t, i))] = v[i];
             __syncthreads();   // all components of the column transformed
-            const r4<R>* kc = kst + (size_t)cl * (L + 1);
+            const r4<R>* kc = LEAN ? reinterpret_cast<const r4<R>*>(F.Khat) + (size_t)(valid ? kx : 0) * (L + 1)
+                                   : kst + (size_t)cl * (L + 1);
             const cx<R>* sx = buf + (6 * cl + 0 + par) * BUF;
             const cx<R>* sy = buf + (6 * cl + 2 + par) * BUF;
             const cx<R>* sz = buf + (6 * cl + 4 + par) * BUF;
@@ -378,7 +384,7 @@ __global__ void __launch_bounds__(ColCfg<R, L, V>::THREADS, ColCfg<R, L, V>::MIN
             }
         }
         __syncthreads();   // products formed: the signal buffers and staged kernel are free
-        if (tid == 0 && has_next) {
+        if (!LEAN && tid == 0 && has_next) {
             fence_async_smem();
             col_issue_k<R, L, V>(films, items, nxt, kst, &bars[1]);
         }

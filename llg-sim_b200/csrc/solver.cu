@@ -299,6 +299,13 @@ static bool env_flag(const char* name) {
     return e && e[0] == '1';
 }
 static bool force_generic() { return env_flag("LLG_B200_GENERIC_FFT"); }
+static int env_int(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    if (!e || !e[0]) return dflt;
+    char* end = nullptr;
+    const long v = std::strtol(e, &end, 10);
+    return (end && *end == 0) ? (int)v : dflt;
+}
 
 // A row radix plan is usable in a segment if it exists and keeps the rows per
 // block of plan 0 (the row work items are shared by the plans).
@@ -359,11 +366,14 @@ struct Engine final : EngineBase {
     std::vector<LaunchGeom> rseg, cseg;
     // each segment's geometry under radix plan 0 / 1 (where the plan exists) and
     // the resident blocks per SM of its kernels; the autotuner picks one
-    std::vector<std::array<LaunchGeom, 2>> rseg_alt, cseg_alt;
-    std::vector<std::array<char, 2>> rseg_has, cseg_has;
+    // (a column segment has 4 forms: 2 * plan + lean)
+    std::vector<std::array<LaunchGeom, 2>> rseg_alt;
+    std::vector<std::array<LaunchGeom, 4>> cseg_alt;
+    std::vector<std::array<char, 2>> rseg_has;
+    std::vector<std::array<char, 4>> cseg_has;
     std::vector<std::array<std::array<int, 4>, 2>> rocc;
     std::vector<std::vector<int>> rseg_films, cseg_films;   // films of each segment
-    std::vector<std::array<int, 2>> cocc;
+    std::vector<std::array<int, 4>> cocc;
 
     int nfilms() const override { return nf; }
     int64_t cells(int f) const override { return grids[f].nx * grids[f].ny; }
@@ -673,22 +683,25 @@ struct Engine final : EngineBase {
                     cseg_films.push_back(fl);
                     cseg.push_back(LaunchGeom{});
                     cseg_alt.push_back({});
-                    cseg_has.push_back({0, 0});
-                    cocc.push_back({1, 1});
+                    cseg_has.push_back({0, 0, 0, 0});
+                    cocc.push_back({1, 1, 1, 1});
                 }
                 const size_t i = col_index[L];
-                LaunchGeom s = geom;
-                s.col_items = d_col_items + sp.second.first;
-                s.n_col_items = (int)sp.second.second;
-                s.fast_col = L;
-                s.col_var = v;
-                int fb = 1, ib = 1, ub = 1, zb = 1, cb = gen_c;
-                if (L) fast_occupancy<R>(0, L, 0, v, &fb, &ib, &ub, &zb, &cb);
-                s.grid_col = balanced(s.n_col_items, cb);
-                cseg_alt[i][v] = s;
-                cseg_has[i][v] = 1;
-                cocc[i][v] = cb;
-                if (v == 0) cseg[i] = s;
+                for (int lean = 0; lean < (L ? 2 : 1); ++lean) {
+                    const int cv = 2 * v + lean;
+                    LaunchGeom s = geom;
+                    s.col_items = d_col_items + sp.second.first;
+                    s.n_col_items = (int)sp.second.second;
+                    s.fast_col = L;
+                    s.col_var = cv;
+                    int fb = 1, ib = 1, ub = 1, zb = 1, cb = gen_c;
+                    if (L) fast_occupancy<R>(0, L, 0, cv, &fb, &ib, &ub, &zb, &cb);
+                    s.grid_col = balanced(s.n_col_items, cb);
+                    cseg_alt[i][cv] = s;
+                    cseg_has[i][cv] = 1;
+                    cocc[i][cv] = cb;
+                    if (cv == 0) cseg[i] = s;
+                }
             }
         }
         if (any_demag && nf == 1) set_l2_window();
@@ -786,11 +799,12 @@ struct Engine final : EngineBase {
             *total = t0 + t1 + t2 + t3;
             return LLG_OK;
         };
-        auto pick = [&](int kind, int L, const std::array<char, 2>& has, auto&& time_plan, int* chosen) -> int {
+        auto pick = [&](int kind, int L, const auto& has, auto&& time_plan, int* chosen) -> int {
             *chosen = 0;
             if (!L) return LLG_OK;
-            if (forced >= 0) {
-                *chosen = has[forced] ? forced : 0;
+            if (forced >= 0) {   // the register plan is fixed; a column keeps its staged form
+                const int f = kind == 1 ? 2 * forced : forced;
+                *chosen = has[f] ? f : 0;
                 return LLG_OK;
             }
             const std::tuple<int, int, int> key{(int)sizeof(R), kind, L};
@@ -804,7 +818,7 @@ struct Engine final : EngineBase {
             }
             if (!tuning) return LLG_OK;
             float best = 1e30f;
-            for (int v = 0; v < 2; ++v) {
+            for (int v = 0; v < (int)has.size(); ++v) {
                 if (!has[v]) continue;
                 float t = 0.f;
                 int rc2;
@@ -833,7 +847,9 @@ struct Engine final : EngineBase {
                 return tune(1, stage, sg, &sg.grid_col, sg.n_col_items, cocc[i][pv], t);
             };
             int v = 0;
-            if ((rc = pick(1, cseg[i].fast_col, cseg_has[i], time_col, &v))) return rc;
+            const int fixed = env_int("LLG_B200_COLUMN_FORM", -1);
+            if (fixed >= 0 && fixed < 4 && cseg[i].fast_col && cseg_has[i][fixed]) v = fixed;
+            else if ((rc = pick(1, cseg[i].fast_col, cseg_has[i], time_col, &v))) return rc;
             float t = 0.f;
             if (tuning && (rc = time_col(v, &t))) return rc;
             cseg[i] = cseg_alt[i][v];

@@ -457,7 +457,8 @@ class Solver:
         return out
 
     def fft_plans(self):
-        """(row plan, column plan) the autotuner chose: 0 default, 1 alternative, -1 generic kernels."""
+        """(row plan, column form) the autotuner chose: row plan 0 default / 1 alternative; column form
+        2 * plan + lean (lean: tables and kernel columns read through L1); -1 generic kernels."""
         r, c = C.c_int32(), C.c_int32()
         _check(lib().llg_solver_fft_plans(self.h, C.byref(r), C.byref(c)))
         return r.value, c.value
