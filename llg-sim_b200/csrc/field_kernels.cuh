@@ -96,6 +96,56 @@ __device__ __forceinline__ void cp3(const R* a, R* o) {
     o[0] = a[0]; o[1] = a[1]; o[2] = a[2];
 }
 
+// Coefficients of the local terms of one film in the solver precision, formed once
+// per work item (the kernels would otherwise reload and convert the FP64 film
+// descriptor for every cell).  The values are the ones the per-cell conversions
+// gave, so results do not change.
+template <typename R>
+struct LocalCoef {
+    R bx, by, bz;                  // Zeeman
+    R exch, ix2, iy2;              // 2A/Ms, 1/dx^2, 1/dy^2
+    R dx, dy, eta;                 // ghost rules
+    R dmi_pref, hx, hy;            // 2D/Ms, 1/(2dx), 1/(2dy)
+    R anis, u0, u1, u2;            // 2Ku/Ms, easy axis
+    bool has_eta, ex_on, dmi_on, anis_on;
+    int nx, ny;
+    const uint8_t* mask;           // null without a geometry mask
+};
+
+template <typename R>
+__device__ __forceinline__ LocalCoef<R> local_coef(const FilmDev& F, bool dmi_on) {
+    LocalCoef<R> c;
+    c.bx = (R)F.bext[0];
+    c.by = (R)F.bext[1];
+    c.bz = (R)F.bext[2];
+    c.exch = (R)F.exch;
+    c.ix2 = (R)F.inv_dx2;
+    c.iy2 = (R)F.inv_dy2;
+    c.dx = (R)F.dx;
+    c.dy = (R)F.dy;
+    c.eta = (R)F.eta;
+    c.dmi_pref = (R)F.dmi_pref;
+    c.hx = (R)F.half_inv_dx;
+    c.hy = (R)F.half_inv_dy;
+    c.anis = (R)F.anis;
+    c.u0 = (R)F.u[0];
+    c.u1 = (R)F.u[1];
+    c.u2 = (R)F.u[2];
+    c.has_eta = F.has_eta != 0;
+    c.ex_on = F.exch != 0.0;
+    c.dmi_on = dmi_on && F.dmi_avail;
+    c.anis_on = F.anis != 0.0;
+    c.nx = F.nx;
+    c.ny = F.ny;
+    c.mask = F.has_mask ? F.mask : nullptr;
+    return c;
+}
+
+template <typename R>
+__device__ __forceinline__ bool coef_inside(const LocalCoef<R>& c, int idx) {
+    return c.mask == nullptr || c.mask[idx] != 0;
+}
+
 // Local effective-field terms at cell (i, j): Zeeman (zeeman.rs:6-12), exchange
 // (exchange.rs:45-222), anisotropy (anisotropy.rs:10-26), DMI (dmi.rs:67-209),
 // accumulated in that order.  With a geometry mask this is the _geom variant
@@ -107,30 +157,29 @@ __device__ __forceinline__ void cp3(const R* a, R* o) {
 // for DMI an edge neighbour is a ghost and a vacuum neighbour a copy).  Divisions
 // by dx^2 and 2 dx are products with reciprocals formed in FP64 on the host.
 template <typename R, typename NB>
-__device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i, int j, bool dmi_on, const R* mc,
-                                               R* b) {
-    const int nx = F.nx, ny = F.ny, idx = j * nx + i;
-    b[0] = (R)0 + (R)F.bext[0];
-    b[1] = (R)0 + (R)F.bext[1];
-    b[2] = (R)0 + (R)F.bext[2];
-    const bool in_c = cell_inside(F, idx);
-    const bool want_ex = F.exch != 0.0 && in_c, want_dmi = dmi_on && F.dmi_avail && in_c;
+__device__ __forceinline__ void local_field_c(const LocalCoef<R>& k, NB&& nb, int i, int j, const R* mc, R* b) {
+    const int nx = k.nx, ny = k.ny, idx = j * nx + i;
+    b[0] = (R)0 + k.bx;
+    b[1] = (R)0 + k.by;
+    b[2] = (R)0 + k.bz;
+    const bool in_c = coef_inside(k, idx);
+    const bool want_ex = k.ex_on && in_c, want_dmi = k.dmi_on && in_c;
     R rim[3], rip[3], rjm[3], rjp[3];
     bool vim = false, vip = false, vjm = false, vjp = false;
     if (want_ex || want_dmi) {
-        vim = nx > 1 && i > 0 && cell_inside(F, idx - 1);
-        vip = nx > 1 && i < nx - 1 && cell_inside(F, idx + 1);
-        vjm = ny > 1 && j > 0 && cell_inside(F, idx - nx);
-        vjp = ny > 1 && j < ny - 1 && cell_inside(F, idx + nx);
+        vim = nx > 1 && i > 0 && coef_inside(k, idx - 1);
+        vip = nx > 1 && i < nx - 1 && coef_inside(k, idx + 1);
+        vjm = ny > 1 && j > 0 && coef_inside(k, idx - nx);
+        vjp = ny > 1 && j < ny - 1 && coef_inside(k, idx + nx);
         if (vim) nb(0, rim);
         if (vip) nb(1, rip);
         if (vjm) nb(2, rjm);
         if (vjp) nb(3, rjp);
     }
-    const R dx = (R)F.dx, dy = (R)F.dy, eta = (R)F.eta;
+    const R dx = k.dx, dy = k.dy, eta = k.eta;
     if (want_ex) {
         // exchange.rs:45-222 with the ghosts of :8-36
-        const bool he = F.has_eta != 0;
+        const bool he = k.has_eta;
         R mim[3], mip[3], mjm[3], mjp[3];
         if (nx == 1) { cp3(mc, mim); cp3(mc, mip); }
         else {
@@ -142,7 +191,7 @@ __device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i,
             if (vjm) cp3(rjm, mjm); else if (he) ghost_y(mc, (R)-1, eta, dy, mjm); else cp3(mc, mjm);
             if (vjp) cp3(rjp, mjp); else if (he) ghost_y(mc, (R)1, eta, dy, mjp); else cp3(mc, mjp);
         }
-        const R coeff = (R)F.exch, ix2 = (R)F.inv_dx2, iy2 = (R)F.inv_dy2;
+        const R coeff = k.exch, ix2 = k.ix2, iy2 = k.iy2;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             R d2x = nx > 1 ? (mip[c] - (R)2 * mc[c] + mim[c]) * ix2 : (R)0;
@@ -150,14 +199,13 @@ __device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i,
             b[c] += coeff * (d2x + d2y);
         }
     }
-    if (F.anis != 0.0) {
+    if (k.anis_on) {
         // anisotropy.rs:10-26
-        const R coeff = (R)F.anis;
-        const R u0 = (R)F.u[0], u1 = (R)F.u[1], u2 = (R)F.u[2];
-        R mdotu = mc[0] * u0 + mc[1] * u1 + mc[2] * u2;
-        b[0] += coeff * mdotu * u0;
-        b[1] += coeff * mdotu * u1;
-        b[2] += coeff * mdotu * u2;
+        const R coeff = k.anis;
+        R mdotu = mc[0] * k.u0 + mc[1] * k.u1 + mc[2] * k.u2;
+        b[0] += coeff * mdotu * k.u0;
+        b[1] += coeff * mdotu * k.u1;
+        b[2] += coeff * mdotu * k.u2;
     }
     if (want_dmi) {
         // dmi.rs:67-209 with the ghosts of :19-52
@@ -172,7 +220,7 @@ __device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i,
             if (j == 0) ghost_y(mc, (R)-1, eta, dy, mjm); else if (vjm) cp3(rjm, mjm); else cp3(mc, mjm);
             if (j == ny - 1) ghost_y(mc, (R)1, eta, dy, mjp); else if (vjp) cp3(rjp, mjp); else cp3(mc, mjp);
         }
-        const R pref = (R)F.dmi_pref, hx = (R)F.half_inv_dx, hy = (R)F.half_inv_dy;
+        const R pref = k.dmi_pref, hx = k.hx, hy = k.hy;
         R dmz_dx = nx > 1 ? (mip[2] - mim[2]) * hx : (R)0;
         R dmz_dy = ny > 1 ? (mjp[2] - mjm[2]) * hy : (R)0;
         R dmx_dx = nx > 1 ? (mip[0] - mim[0]) * hx : (R)0;
@@ -181,6 +229,12 @@ __device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i,
         b[1] += pref * dmz_dy;
         b[2] += -pref * (dmx_dx + dmy_dy);
     }
+}
+
+template <typename R, typename NB>
+__device__ __forceinline__ void local_field_nb(const FilmDev& F, NB&& nb, int i, int j, bool dmi_on, const R* mc,
+                                               R* b) {
+    local_field_c<R>(local_coef<R>(F, dmi_on), nb, i, j, mc, b);
 }
 
 template <typename R>

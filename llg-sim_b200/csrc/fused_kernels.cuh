@@ -152,6 +152,7 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<
             for (int q = 0; q < 6; ++q) cq[q] = q < sf.nterm ? (R)(dt * sf.a[q]) : (R)0;
             const R cs = (R)(dt * sf.a[nq]);   // k_s coefficient
             const R Ms = (R)F.ms;
+            const LocalCoef<R> cf = local_coef<R>(F, si.dmi != 0);
             for (int e = tid; e < NV; e += C::THREADS) {
                 const int c0 = e * W, r = c0 / L, i0 = c0 - r * L, j = j0 + r;
                 if (j >= ny) {   // rows past the film are zero in the forward transform
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<
                         }
                     };
                     R b[3];
-                    local_field_nb<R>(F, nb, i, j, si.dmi != 0, mc, b);
+                    local_field_c<R>(cf, nb, i, j, mc, b);
                     if (do_fft) {
 #pragma unroll
                         for (int c = 0; c < 3; ++c) b[c] += *slot(c, r, i);
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<
 #pragma unroll
                 for (int l = 0; l < W; ++l) {
                     R v3[3] = {a[0].v[l], a[1].v[l], a[2].v[l]};
-                    if (cell_inside(F, base + l)) normalize3(v3);
+                    if (coef_inside(cf, base + l)) normalize3(v3);
                     else { v3[0] = (R)0; v3[1] = (R)0; v3[2] = (R)0; }   // vacuum pinned at m = 0
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {

@@ -17,10 +17,16 @@ __global__ void __launch_bounds__(256, 4) k_stage_torque(const FilmDev* __restri
                                                           const WorkItem* __restrict__ items, int nitems, int cpi,
                                                           EvalSpec spec) {
     const long long total = (long long)nitems * cpi;
+    int coef_film = -1;
+    LocalCoef<R> cf;
     for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < total;
          v += (long long)gridDim.x * blockDim.x) {
         const WorkItem w = items[v / cpi];
         const FilmDev& F = films[w.film];
+        if (w.film != coef_film) {   // coefficients of the local terms, once per film
+            cf = local_coef<R>(F, spec.dmi != 0);
+            coef_film = w.film;
+        }
         StepState* st = F.st;
         if (skip_item(spec, st)) continue;   // uniform over the warp (one item per warp)
         const int nx = F.nx, ny = F.ny, n = nx * ny;
@@ -33,7 +39,9 @@ __global__ void __launch_bounds__(256, 4) k_stage_torque(const FilmDev* __restri
             R* __restrict__ kout = kbuf<R>(F, spec.k_out, cur);
             R mc[3], b[3];
             ld3(msb, n, idx, mc);
-            local_field<R>(F, msb, i, j, spec.dmi != 0, mc, b);
+            local_field_c<R>(
+                cf, [&](int d, R* o) { ld3(msb, n, d == 0 ? idx - 1 : d == 1 ? idx + 1 : d == 2 ? idx - nx : idx + nx, o); },
+                i, j, mc, b);
             if (spec.demag && F.demag_mat) {
                 const R* bd = reinterpret_cast<const R*>(F.bdem);
                 b[0] += bd[idx];
