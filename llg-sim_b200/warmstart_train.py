@@ -49,14 +49,19 @@ def init_params(seed):
 
 
 def relax_dataset(n, size, seed, chunk, max_steps, torque, log, budget_s=None):
-    """Relaxed films on the host: m0 and m_relaxed as FP32 SoA [n][3][size*size],
-    masks uint8 [n][size*size], B_ext [n][3], accepted steps [n].  With budget_s, no
-    new chunk starts after that many seconds (the films done so far are returned)."""
+    """Relaxed films, kept on the GPU as they are produced (torch tensors used as
+    device arrays): m0 and m_relaxed FP32 SoA [n][3][size*size], masks uint8
+    [n][size*size]; B_ext [n][3] and accepted steps [n] on the host.  Host memory
+    holds one film at a time.  With budget_s, no new chunk starts after that many
+    seconds (the films done so far are returned)."""
+    import torch
+
     films, rx = W.holey_film_batch(n, size, seed=seed)
     hw = size * size
-    m0 = np.empty((n, 3, hw), dtype=np.float32)
-    mrel = np.empty((n, 3, hw), dtype=np.float32)
-    masks = np.empty((n, hw), dtype=np.uint8)
+    dev = "cuda"
+    m0 = torch.empty((n, 3, hw), dtype=torch.float32, device=dev)
+    mrel = torch.empty((n, 3, hw), dtype=torch.float32, device=dev)
+    masks = torch.empty((n, hw), dtype=torch.uint8, device=dev)
     bext = np.empty((n, 3))
     steps = np.empty(n, dtype=np.int64)
     t_start = time.time()
@@ -71,8 +76,8 @@ def relax_dataset(n, size, seed, chunk, max_steps, torque, log, budget_s=None):
             m = L.init_random(f.n, seed * 1000003 + c0 + i)
             m[f.mask == 0] = 0.0
             b.set_state(i, m)
-            m0[c0 + i] = m.T
-            masks[c0 + i] = f.mask
+            m0[c0 + i] = torch.from_numpy(np.ascontiguousarray(m.T, dtype=np.float32))
+            masks[c0 + i] = torch.from_numpy(np.ascontiguousarray(f.mask, dtype=np.uint8))
             bext[c0 + i] = f.b_ext
         st = L.RelaxSettings.default(torque_threshold=torque, max_err=rx["max_err"], headroom=rx["headroom"],
                                      dt_min=rx["dt_min"], dt_max=rx["dt_max"], max_accepted_steps=max_steps)
@@ -80,7 +85,7 @@ def relax_dataset(n, size, seed, chunk, max_steps, torque, log, budget_s=None):
         t0 = time.time()
         reps = b.relax(P, L.FULL, st)
         for i in range(len(part)):
-            mrel[c0 + i] = b.get_state(i).T
+            mrel[c0 + i] = torch.from_numpy(np.ascontiguousarray(b.get_state(i).T, dtype=np.float32))
             steps[c0 + i] = reps[i].accepted_steps
         s = steps[c0:c0 + len(part)]
         log(f"relaxed films {c0}..{c0 + len(part) - 1} in {time.time() - t0:.1f} s, steps {int(s.mean())} mean / "
@@ -93,13 +98,11 @@ def relax_dataset(n, size, seed, chunk, max_steps, torque, log, budget_s=None):
 def train(data, size, epochs, batch, lr, log, seed=0, holdout=0.02, params=None):
     import torch
 
-    m0, masks, bext, mrel, _ = data
-    n = m0.shape[0]
+    d_m0, d_k, bext, d_t, _ = data
+    n = d_m0.shape[0]
     dev = "cuda"
-    d_m0 = torch.from_numpy(m0).to(dev)
-    d_t = torch.from_numpy(mrel).to(dev)
-    d_k = torch.from_numpy(masks).to(dev)
     d_b = torch.from_numpy(np.ascontiguousarray(bext, dtype=np.float64)).to(dev)
+    inside = d_k.sum(dim=1).cpu().numpy().astype(np.float64)   # film cells per film
     rng = np.random.default_rng(seed)
     order = rng.permutation(n)
     n_hold = max(1, int(round(holdout * n))) if n > 8 else 0
@@ -130,7 +133,7 @@ def train(data, size, epochs, batch, lr, log, seed=0, holdout=0.02, params=None)
             idx = hold[b0:b0 + batch]
             k, ptrs = gather(idx)
             loss, _ = tr.gradients(k, size, size, *ptrs)
-            c = float(masks[idx].astype(bool).sum())
+            c = float(inside[idx].sum())
             tot += loss * c
             cells += c
         return tot / max(cells, 1.0)
@@ -196,8 +199,12 @@ def main():
     log(f"dataset: {n_rel} films relaxed in {t_data:.1f} s")
     steps_all = data[4]
     if args.drop_capped:
+        import torch
+
         keep = steps_all < args.max_steps
-        data = tuple(x[keep] for x in data)
+        kt = torch.from_numpy(np.nonzero(keep)[0]).to("cuda")
+        m0, masks, bext, mrel, st = data
+        data = (m0[kt], masks[kt], bext[keep], mrel[kt], st[keep])
         log(f"training on {int(keep.sum())} films that reached the torque ({int((~keep).sum())} at the cap dropped)")
     init = np.load(args.init) if args.init else None
     t1 = time.time()
