@@ -159,22 +159,18 @@ cudaError_t net_apply(Net* net, const R* m_in, R* m_out, const uint8_t* mask, co
     if (e != cudaSuccess) return e;
     k_ws_input<R><<<(unsigned)std::min<long long>((cells + 255) / 256, 148 * 16), 256, 0, s>>>(m_in, mask, net->bext,
                                                                                               nimg, hw, net->x0);
-    const unsigned grid = (unsigned)((cells + kTile - 1) / kTile);
     const __nv_bfloat16* cur = net->x0;
     for (int l = 0; l < kLayers; ++l) {
         const Layer& L = net->L[l];
-        const size_t smem = conv_smem_bytes(L.cin, L.npad);
         if (l < kLayers - 1) {
             __nv_bfloat16* nxt = net->h[l & 1];
-            k_conv3x3_tc<kCh, EPI_HIDDEN, R><<<grid, kTile, smem, s>>>(cur, nimg, ny, nx, L, nxt, nullptr, nullptr,
-                                                                        nullptr, nullptr, net->err, net->spin);
+            e = conv_launch<kCh, EPI_HIDDEN, R>(cur, nimg, ny, nx, L, nxt, nullptr, nullptr, nullptr, nullptr, net->err,
+                                                net->spin, s);
             cur = nxt;
         } else {
-            k_conv3x3_tc<kNout, EPI_FINAL_NORM, R><<<grid, kTile, smem, s>>>(cur, nimg, ny, nx, L, nullptr, m_out,
-                                                                              nullptr, mask, nullptr, net->err,
-                                                                              net->spin);
+            e = conv_launch<kNout, EPI_FINAL_NORM, R>(cur, nimg, ny, nx, L, nullptr, m_out, nullptr, mask, nullptr,
+                                                      net->err, net->spin, s);
         }
-        e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

@@ -28,6 +28,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cstdlib>
+
 #include "async_copy.cuh"
 
 namespace llg {
@@ -255,6 +258,276 @@ __global__ void __launch_bounds__(kTile) k_conv3x3_tc(const __nv_bfloat16* __res
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, kCols);
+}
+
+// Per-cell epilogue shared by the one-shot and the pipelined convolution.
+template <int NCOL, int EPI, typename R>
+__device__ __forceinline__ void conv_epilogue(const float (&acc)[NCOL], long long p, long long hw, const Layer& L,
+                                              __nv_bfloat16* __restrict__ y, R* __restrict__ m_out,
+                                              float* __restrict__ out32, const uint8_t* __restrict__ mask,
+                                              const __nv_bfloat16* __restrict__ act) {
+    if constexpr (EPI == EPI_HIDDEN || EPI == EPI_DGRAD) {
+        alignas(16) __nv_bfloat16 o[NCOL];
+        if constexpr (EPI == EPI_DGRAD) {
+            alignas(16) __nv_bfloat16 a[NCOL];
+#pragma unroll
+            for (int q = 0; q < NCOL / 8; ++q)
+                reinterpret_cast<uint4*>(a)[q] = reinterpret_cast<const uint4*>(act + p * NCOL)[q];
+#pragma unroll
+            for (int c = 0; c < NCOL; ++c) o[c] = __float2bfloat16(__bfloat162float(a[c]) > 0.0f ? acc[c] : 0.0f);
+        } else {
+#pragma unroll
+            for (int c = 0; c < NCOL; ++c) {
+                float v = acc[c] + L.b[c];
+                if (L.relu) v = fmaxf(v, 0.0f);
+                o[c] = __float2bfloat16(v);
+            }
+        }
+        uint4* dst = reinterpret_cast<uint4*>(y + p * NCOL);
+#pragma unroll
+        for (int q = 0; q < NCOL / 8; ++q) dst[q] = reinterpret_cast<const uint4*>(o)[q];
+    } else if constexpr (EPI == EPI_FINAL_RAW) {
+        *reinterpret_cast<float4*>(out32 + p * 4) = make_float4(acc[0] + L.b[0], acc[1] + L.b[1], acc[2] + L.b[2], 0.0f);
+    } else {
+        const int img = (int)(p / hw);
+        const long long cell = p - (long long)img * hw;
+        float v0 = acc[0] + L.b[0], v1 = acc[1] + L.b[1], v2 = acc[2] + L.b[2];
+        const bool inside = mask == nullptr || mask[p] != 0;
+        const float nn = v0 * v0 + v1 * v1 + v2 * v2;
+        if (!inside) {
+            v0 = v1 = v2 = 0.0f;
+        } else if (nn > 0.0f) {
+            const float inv = 1.0f / sqrtf(nn);
+            v0 *= inv; v1 *= inv; v2 *= inv;
+        } else {
+            v0 = 0.0f; v1 = 0.0f; v2 = 1.0f;   // normalize(0) = +z (vec3.rs:21-25)
+        }
+        R* mo = m_out + (size_t)img * 3 * hw;
+        mo[cell] = (R)v0;
+        mo[hw + cell] = (R)v1;
+        mo[2 * hw + cell] = (R)v2;
+    }
+}
+
+// Pipelined convolution for images up to kHaloW cells wide: a persistent CTA loads
+// the layer's weights once and walks 128-cell tiles.  For each tile the cells it
+// reads (the tile and one image row plus one cell on either side) are one
+// contiguous NHWC range, fetched by a 1-D bulk copy (cp.async.bulk, this GPU's
+// memory, no multicast) into one of two halo buffers while the previous tile is
+// processed; the im2col rows are built from shared memory; the MMAs of a tile
+// accumulate into one of two TMEM accumulators, so the epilogue of tile k-1 runs
+// while the tensor cores work on tile k.  The MMA sequence of a tile is the one
+// of k_conv3x3_tc (same operands, same order), so both kernels give the same bits.
+constexpr int kHaloW = 256;
+constexpr int kHaloCells = kTile + 2 * kHaloW + 2;
+
+template <int CIN>
+__host__ __device__ constexpr size_t conv_pipe_smem_bytes(int npad) {
+    return (size_t)npad * 9 * CIN * 2 + (size_t)kTile * 9 * CIN * 2 + 2 * (size_t)kHaloCells * CIN * 2;
+}
+
+template <int NCOL, int EPI, typename R, int CIN>
+__global__ void __launch_bounds__(kTile) k_conv3x3_pipe(const __nv_bfloat16* __restrict__ x, int nimg, int H, int W,
+                                                        Layer L, __nv_bfloat16* __restrict__ y,
+                                                        R* __restrict__ m_out, float* __restrict__ out32,
+                                                        const uint8_t* __restrict__ mask,
+                                                        const __nv_bfloat16* __restrict__ act, int* err,
+                                                        long long spin) {
+    constexpr int K = 9 * CIN;
+    constexpr uint32_t sbo = (uint32_t)K * 16;
+    constexpr uint32_t kCols = 2 * (NCOL < 32 ? 32 : NCOL);
+    constexpr uint32_t kAcc = NCOL < 32 ? 32 : NCOL;   // column offset of the second accumulator
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar_halo[2], bar_mma;
+    __shared__ uint32_t tmem_base;
+    unsigned char* Bs = smem;
+    unsigned char* As = Bs + (size_t)L.npad * K * 2;
+    unsigned char* Hs = As + (size_t)kTile * K * 2;   // two halo buffers of kHaloCells * CIN bf16
+    const int t = threadIdx.x, warp = t >> 5;
+    const long long hw = (long long)H * W, total = (long long)nimg * hw;
+    const long long ntiles = (total + kTile - 1) / kTile;
+
+    if (warp == 0) tmem_alloc(&tmem_base, kCols);
+    if (t == 0) {
+        mbar_init(&bar_halo[0], 1);
+        mbar_init(&bar_halo[1], 1);
+        mbar_init(&bar_mma, 1);
+        mbar_init_fence();
+    }
+    // weights, K-major core matrices
+    for (int c = t; c < L.npad * (K / 8); c += kTile) {
+        const int n = c / (K / 8), kc = c - n * (K / 8);
+        const uint4 v = reinterpret_cast<const uint4*>(L.w + (size_t)n * K)[kc];
+        *reinterpret_cast<uint4*>(Bs + (size_t)(n >> 3) * sbo + (size_t)kc * 128 + (size_t)(n & 7) * 16) = v;
+    }
+    __syncthreads();
+    const uint32_t tmem = tmem_base;
+    auto halo_range = [&](long long tile, long long* lo, long long* cnt) {
+        const long long p0 = tile * kTile;
+        const long long a = p0 - W - 1 < 0 ? 0 : p0 - W - 1;
+        long long b = p0 + kTile + W + 1;
+        if (b > total) b = total;
+        *lo = a;
+        *cnt = b - a;
+    };
+    auto issue_halo = [&](long long tile, int buf) {
+        long long lo, cnt;
+        halo_range(tile, &lo, &cnt);
+        const uint32_t bytes = (uint32_t)(cnt * CIN * 2);
+        mbar_arrive_expect_tx(&bar_halo[buf], bytes);
+        bulk_copy_g2s(Hs + (size_t)buf * kHaloCells * CIN * 2, x + lo * CIN, bytes, &bar_halo[buf]);
+    };
+    // Outstanding asynchronous work, tracked identically by every thread (the tile
+    // sequence is fixed): the phase parity of the last copy issued into each halo
+    // buffer that has not been waited for (-1: none), and of the last MMA commit.
+    int halo_pending[2] = {-1, -1};
+    int mma_pending = -1;
+    long long tile = blockIdx.x;
+    if (tile < ntiles) {
+        if (t == 0) {
+            fence_async_smem();
+            issue_halo(tile, 0);
+        }
+        halo_pending[0] = 0;
+    }
+    const uint32_t idesc = instr_desc_bf16(kTile, L.npad, false, false);
+    bool ok = true;
+    int k = 0;
+    long long prev = -1;
+    for (; tile < ntiles; tile += gridDim.x, ++k) {
+        const int hb = k & 1;
+        ok = mbar_wait_n(&bar_halo[hb], (uint32_t)((k >> 1) & 1), spin);
+        if (!ok) break;
+        halo_pending[hb] = -1;
+        if (mma_pending >= 0) {   // the MMAs of the previous tile have read the im2col buffer
+            ok = mbar_wait_n(&bar_mma, (uint32_t)mma_pending, spin);
+            if (!ok) break;
+            mma_pending = -1;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        }
+        // the other halo buffer was read by the previous tile's im2col build (before
+        // the previous barrier): refill it with the next tile's range
+        if (tile + gridDim.x < ntiles) {
+            if (t == 0) {
+                fence_async_smem();
+                issue_halo(tile + gridDim.x, hb ^ 1);
+            }
+            halo_pending[hb ^ 1] = ((k + 1) >> 1) & 1;
+        }
+        // im2col row of cell p from the halo (zero outside the image)
+        {
+            long long lo, cnt;
+            halo_range(tile, &lo, &cnt);
+            const unsigned char* hsrc = Hs + (size_t)hb * kHaloCells * CIN * 2;
+            const long long p = tile * kTile + t;
+            const bool valid = p < total;
+            const int img = valid ? (int)(p / hw) : 0;
+            const int rem = valid ? (int)(p - (long long)img * hw) : 0;
+            const int yy = rem / W, xx = rem - (rem / W) * W;
+            unsigned char* arow = As + (size_t)(t >> 3) * sbo + (size_t)(t & 7) * 16;
+#pragma unroll
+            for (int tap = 0; tap < 9; ++tap) {
+                const int sy = yy + tap / 3 - 1, sx = xx + tap % 3 - 1;
+                const bool in = valid && sy >= 0 && sy < H && sx >= 0 && sx < W;
+                const long long q = p + (long long)(tap / 3 - 1) * W + (tap % 3 - 1);
+                const uint4* src = reinterpret_cast<const uint4*>(hsrc + (in ? (q - lo) : 0) * CIN * 2);
+#pragma unroll
+                for (int g = 0; g < CIN / 8; ++g) {
+                    const uint4 v = in ? src[g] : make_uint4(0u, 0u, 0u, 0u);
+                    *reinterpret_cast<uint4*>(arow + (size_t)((tap * CIN + g * 8) >> 3) * 128) = v;
+                }
+            }
+        }
+        fence_async_smem();
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc_col = (uint32_t)hb * kAcc;
+        if (t == 0) {
+            const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs);
+            for (int kk = 0; kk < K / 16; ++kk)
+                mma_bf16(tmem + acc_col, smem_desc(a0 + kk * 256, 128, sbo), smem_desc(b0 + kk * 256, 128, sbo), idesc,
+                         kk > 0 ? 1u : 0u);
+            mma_commit(&bar_mma);
+        }
+        mma_pending = k & 1;
+        // epilogue of the previous tile while the tensor cores work on this one
+        if (prev >= 0) {
+            float acc[NCOL];
+            tmem_ld<NCOL>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(hb ^ 1) * kAcc, acc);
+            const long long p = prev * kTile + t;
+            if (p < total) conv_epilogue<NCOL, EPI, R>(acc, p, hw, L, y, m_out, out32, mask, act);
+        }
+        prev = tile;
+    }
+    if (ok && mma_pending >= 0) {
+        ok = mbar_wait_n(&bar_mma, (uint32_t)mma_pending, spin);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (ok) {
+            mma_pending = -1;
+            float acc[NCOL];
+            tmem_ld<NCOL>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((k - 1) & 1) * kAcc, acc);
+            const long long p = prev * kTile + t;
+            if (p < total) conv_epilogue<NCOL, EPI, R>(acc, p, hw, L, y, m_out, out32, mask, act);
+        }
+    }
+    if (!ok) {
+        if (t == 0) atomicExch(err, 1);
+        // one more bounded wait for the copies and MMAs still in flight, so that none
+        // writes shared memory or TMEM after the CTA has released them
+        if (mma_pending >= 0) mbar_wait(&bar_mma, (uint32_t)mma_pending);
+        for (int b = 0; b < 2; ++b)
+            if (halo_pending[b] >= 0) mbar_wait(&bar_halo[b], (uint32_t)halo_pending[b]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, kCols);
+}
+
+// Launch of one convolution layer: the pipelined kernel for images up to kHaloW
+// cells wide, the one-shot kernel otherwise (LLG_B200_CONV_ONESHOT=1 selects the
+// one-shot kernel everywhere; both give the same bits).
+inline bool conv_oneshot_forced() {
+    const char* e = std::getenv("LLG_B200_CONV_ONESHOT");
+    return e && e[0] == '1';
+}
+
+template <int NCOL, int EPI, typename R>
+cudaError_t conv_launch(const __nv_bfloat16* x, int nimg, int H, int W, const Layer& L, __nv_bfloat16* y, R* m_out,
+                        float* out32, const uint8_t* mask, const __nv_bfloat16* act, int* err, long long spin,
+                        cudaStream_t s) {
+    const long long cells = (long long)nimg * H * W;
+    if (cells <= 0) return cudaSuccess;
+    const long long ntiles = (cells + kTile - 1) / kTile;
+    if (W <= kHaloW && (L.cin == 16 || L.cin == 32) && !conv_oneshot_forced()) {
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const unsigned grid = (unsigned)std::min<long long>(ntiles, nsm);
+        if (L.cin == 32) {
+            const size_t smem = conv_pipe_smem_bytes<32>(L.npad);
+            cudaError_t e = cudaFuncSetAttribute(k_conv3x3_pipe<NCOL, EPI, R, 32>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            k_conv3x3_pipe<NCOL, EPI, R, 32><<<grid, kTile, smem, s>>>(x, nimg, H, W, L, y, m_out, out32, mask, act,
+                                                                        err, spin);
+        } else {
+            const size_t smem = conv_pipe_smem_bytes<16>(L.npad);
+            cudaError_t e = cudaFuncSetAttribute(k_conv3x3_pipe<NCOL, EPI, R, 16>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            k_conv3x3_pipe<NCOL, EPI, R, 16><<<grid, kTile, smem, s>>>(x, nimg, H, W, L, y, m_out, out32, mask, act,
+                                                                        err, spin);
+        }
+        return cudaGetLastError();
+    }
+    const size_t smem = conv_smem_bytes(L.cin, L.npad);
+    cudaError_t e = cudaFuncSetAttribute(k_conv3x3_tc<NCOL, EPI, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    k_conv3x3_tc<NCOL, EPI, R><<<(unsigned)ntiles, kTile, smem, s>>>(x, nimg, H, W, L, y, m_out, out32, mask, act, err,
+                                                                     spin);
+    return cudaGetLastError();
 }
 
 // Network input of image f from SoA planes m (R), mask and the image's field.

@@ -464,22 +464,19 @@ cudaError_t trainer_backprop(Trainer* tr, int nimg, int ny, int nx, const float*
     if (e != cudaSuccess) return e;
     k_ws_input<float><<<(unsigned)std::min<long long>((P + 255) / 256, 148 * 16), 256, 0, s>>>(m0, mask, bext, nimg,
                                                                                              hw, tr->x0);
-    const unsigned grid = (unsigned)((P + kTile - 1) / kTile);
     // forward
     const __nv_bfloat16* cur = tr->x0;
     for (int l = 0; l < kLayers; ++l) {
         const Layer L = fwd_layer(tr, l);
-        const size_t smem = conv_smem_bytes(L.cin, L.npad);
         if (l < kLayers - 1) {
-            k_conv3x3_tc<kCh, EPI_HIDDEN, float><<<grid, kTile, smem, s>>>(cur, nimg, ny, nx, L, tr->h[l], nullptr,
-                                                                           nullptr, nullptr, nullptr, tr->err,
-                                                                           tr->spin);
+            e = conv_launch<kCh, EPI_HIDDEN, float>(cur, nimg, ny, nx, L, tr->h[l], nullptr, nullptr, nullptr, nullptr,
+                                                    tr->err, tr->spin, s);
             cur = tr->h[l];
         } else {
-            k_conv3x3_tc<kNout, EPI_FINAL_RAW, float><<<grid, kTile, smem, s>>>(cur, nimg, ny, nx, L, nullptr, nullptr,
-                                                                                tr->out32, nullptr, nullptr, tr->err,
-                                                                                tr->spin);
+            e = conv_launch<kNout, EPI_FINAL_RAW, float>(cur, nimg, ny, nx, L, nullptr, nullptr, tr->out32, nullptr,
+                                                         nullptr, tr->err, tr->spin, s);
         }
+        if (e != cudaSuccess) return e;
     }
     // loss and its gradient (layer 5 output gradient, 16 channels, in g[0])
     k_cos_loss<<<tr->loss_blocks, kRedThreads, 0, s>>>(tr->out32, target, mask, nimg, hw, tr->g[0], tr->lpart);
@@ -513,8 +510,9 @@ cudaError_t trainer_backprop(Trainer* tr, int nimg, int ny, int nx, const float*
         if (l > 0) {
             // g_{l-1} = conv(g_l, W_l transposed / flipped) * (h_{l-1} > 0)
             const Layer Ld{tr->wd[l], nullptr, D.cout_pad, D.cin_pad, D.cin_pad, 0};
-            k_conv3x3_tc<kCh, EPI_DGRAD, float><<<grid, kTile, conv_smem_bytes(Ld.cin, Ld.npad), s>>>(
-                gl, nimg, ny, nx, Ld, tr->g[gi ^ 1], nullptr, nullptr, nullptr, tr->h[l - 1], tr->err, tr->spin);
+            e = conv_launch<kCh, EPI_DGRAD, float>(gl, nimg, ny, nx, Ld, tr->g[gi ^ 1], nullptr, nullptr, nullptr,
+                                                   tr->h[l - 1], tr->err, tr->spin, s);
+            if (e != cudaSuccess) return e;
             gi ^= 1;
         }
     }

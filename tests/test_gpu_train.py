@@ -69,6 +69,20 @@ def test_gradients_match_fp64_restatement(gpu, nimg, ny, nx, holes):
     tr.close()
 
 
+def test_pipelined_and_oneshot_convolutions_give_the_same_gradients(gpu, monkeypatch):
+    ny, nx = 40, 72
+    params = ref.random_params(6)
+    m, mask, b, t = _batch(2, ny, nx, 8, True)
+    d = _device(m, mask, b, t, ny, nx)
+    tr = gpu.WarmStartTrainer(params, 2 * ny * nx)
+    l1, g1 = tr.gradients(2, ny, nx, *_ptrs(d))
+    monkeypatch.setenv("LLG_B200_CONV_ONESHOT", "1")
+    l2, g2 = tr.gradients(2, ny, nx, *_ptrs(d))
+    monkeypatch.delenv("LLG_B200_CONV_ONESHOT")
+    assert l1 == l2 and np.array_equal(g1, g2)
+    tr.close()
+
+
 def test_adam_steps_reduce_the_loss(gpu):
     ny = nx = 32
     params = ref.random_params(8)

@@ -102,3 +102,19 @@ def test_trained_warm_start_shortens_relax(gpu):
         b.close()
     net.close()
     assert steps[True] < steps[False]
+
+
+@pytest.mark.parametrize("nimg,ny,nx", [(3, 128, 128), (2, 37, 200), (1, 9, 256)])
+def test_pipelined_convolution_gives_the_same_bits(gpu, monkeypatch, nimg, ny, nx):
+    """The persistent, halo-staged convolution (images up to 256 cells wide) and the
+    one-shot kernel (LLG_B200_CONV_ONESHOT=1) issue the same MMAs on the same
+    operands: identical proposals."""
+    params = ref.random_params(9)
+    net = gpu.WarmStartNet(params)
+    m, mask, b = _inputs(nimg, ny, nx, 21, True)
+    piped = net.forward(m, mask, b, ny, nx)
+    monkeypatch.setenv("LLG_B200_CONV_ONESHOT", "1")
+    oneshot = net.forward(m, mask, b, ny, nx)
+    monkeypatch.delenv("LLG_B200_CONV_ONESHOT")
+    assert np.array_equal(piped, oneshot)
+    net.close()
