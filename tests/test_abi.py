@@ -99,3 +99,10 @@ def test_struct_layouts_match_header(gpu, tmp_path):
         assert got[(cname, "size")] == C.sizeof(cls), cname
         for fname, _ in cls._fields_:
             assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
+
+
+def test_trainer_parameter_layout_matches_the_network():
+    import warmstart_train as T
+
+    p = T.init_params(3)
+    assert p.dtype == np.float32 and p.size == sum(co * 9 * ci + co for ci, co in T.LAYERS)
