@@ -472,6 +472,21 @@ def amr_leg(L, reps=5):
         L.allfft_demag(op, mat, mf, None, bg)
     out["allfft_ms"] = (time.perf_counter() - t0) / reps * 1e3
     out["allfft_io_bytes"] = int(mf.nbytes * 2 + nx * ny * 24)
+    # the same on resident device arrays (an AMR code that keeps its hierarchy on the GPU)
+    import torch
+
+    d_m = torch.from_numpy(np.ascontiguousarray(mf)).cuda()
+    d_bf = torch.empty_like(d_m)
+    d_bc = torch.empty((nx * ny, 3), dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream()
+    L.allfft_demag_device(op, mat, d_m.data_ptr(), 0, bg, d_bf.data_ptr(), d_bc.data_ptr(), st.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        L.allfft_demag_device(op, mat, d_m.data_ptr(), 0, bg, d_bf.data_ptr(), d_bc.data_ptr(), st.cuda_stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    out["allfft_device_ms"] = e0.elapsed_time(e1) / reps
     op.close()
     try:
         import oracle as O
@@ -600,6 +615,7 @@ def compact_legs(batch, flow, warm, amr, sp4r, mini):
         out["warm_start_c5"] = _r({k: warm[k] for k in warm if k not in ("workload", "weights", "films")})
     if amr:
         out["amr_demag"] = _r({"coarse_fft_ms": amr["coarse_fft_ms"], "allfft_ms": amr["allfft_ms"],
+                               "allfft_device_ms": amr.get("allfft_device_ms"),
                                "cpu_coarse_fft_ms": amr.get("cpu_coarse_fft_ms")})
     if sp4r:
         out["sp4"] = _r({"fp32_wall_s": sp4r["fp32"]["wall_s"], "fp64_wall_s": sp4r["fp64"]["wall_s"],

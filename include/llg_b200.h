@@ -374,6 +374,12 @@ int llg_coarse_fft_demag(llg_amr_demag* h, const llg_material* mat, const double
  * fine_mask is 0 (NULL: no mask), bilinear samples at the base-grid cell centres. */
 int llg_amr_allfft_demag(llg_demag_op* fine_op, const llg_material* mat, const double* m_fine,
                          const uint8_t* fine_mask, const llg_grid* base, double* b_fine, double* b_coarse);
+/* The same on DEVICE arrays (m_fine, fine_mask or NULL, b_fine, b_coarse), for an
+ * AMR code that keeps its hierarchy on the GPU: no host transfer and no
+ * allocation, asynchronous on `stream` (cudaStream_t as void*, NULL = default). */
+int llg_amr_allfft_demag_device(llg_demag_op* fine_op, const llg_material* mat, const double* d_m_fine,
+                                const uint8_t* d_fine_mask, const llg_grid* base, double* d_b_fine,
+                                double* d_b_coarse, void* stream);
 
 /* ---------------- OVF 2.0 writers (ovf.rs:17-251) ----------------
  * OvfMeta (ovf.rs:17-45): title, "# Desc:" lines, value labels and units.

@@ -514,4 +514,32 @@ int llg_amr_allfft_demag(llg_demag_op* fine_op, const llg_material* mat, const d
     return done(LLG_OK);
 }
 
+// The AllFft demag on device arrays: no host transfer and no allocation (the
+// operator's own buffers hold the transforms), asynchronous on `stream`.
+int llg_amr_allfft_demag_device(llg_demag_op* fine_op, const llg_material* mat, const double* d_m_fine,
+                                const uint8_t* d_fine_mask, const llg_grid* base, double* d_b_fine,
+                                double* d_b_coarse, void* stream) {
+    if (!fine_op || !mat || !d_m_fine || !base || !d_b_fine || !d_b_coarse) return fail(LLG_ERR_INVALID, "null argument");
+    int device = 0, pbx = 0, pby = 0;
+    llg_grid fg{};
+    llg::demag_op_info(fine_op, &device, &fg, &pbx, &pby);
+    if (pbx || pby) return fail(LLG_ERR_INVALID, "the AllFft demag uses open boundaries (pbc 0, 0)");
+    if (base->nx < 1 || base->ny < 1 || !(base->dx > 0) || !(base->dy > 0)) return fail(LLG_ERR_INVALID, "bad base grid");
+    AMR_TRY(cudaSetDevice(device));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const long long nf = fg.nx * fg.ny, nb = base->nx * base->ny;
+    if (!mat->demag) {
+        AMR_TRY(cudaMemsetAsync(d_b_fine, 0, sizeof(double) * 3 * (size_t)nf, s));
+        AMR_TRY(cudaMemsetAsync(d_b_coarse, 0, sizeof(double) * 3 * (size_t)nb, s));
+        return LLG_OK;
+    }
+    int rc;
+    if ((rc = llg::demag_op_apply_device(fine_op, mat->ms, d_m_fine, d_b_fine, s))) return rc;
+    if (d_fine_mask) k_zero_vacuum<<<kGrid, 256, 0, s>>>(d_b_fine, d_fine_mask, nf);
+    k_sample_grid<<<kGrid, 256, 0, s>>>(d_b_fine, fg.nx, fg.ny, fg.dx, fg.dy, base->nx, base->ny, base->dx, base->dy,
+                                        d_b_coarse);
+    if (cudaGetLastError() != cudaSuccess) return fail(LLG_ERR_CUDA, "AllFft demag kernels");
+    return LLG_OK;
+}
+
 }  // extern "C"

@@ -225,6 +225,7 @@ def lib():
             "llg_amr_restrict_m": (C.c_int, [vp, dp, i32, P(_AmrPatch), dp]),
             "llg_coarse_fft_demag": (C.c_int, [vp, P(_Material), dp, i32, P(_AmrPatch), dp, dp]),
             "llg_amr_allfft_demag": (C.c_int, [vp, P(_Material), dp, vp, P(_Grid), dp, dp]),
+            "llg_amr_allfft_demag_device": (C.c_int, [vp, P(_Material), vp, vp, P(_Grid), vp, vp, vp]),
             "llg_warmstart_param_count": (i64, []),
             "llg_warmstart_create": (C.c_int, [vp, P(C.c_float), i64, P(vp)]),
             "llg_warmstart_destroy": (C.c_int, [vp]),
@@ -763,6 +764,16 @@ def allfft_demag(fine_op, material, m_fine, fine_mask, base_grid):
     _check(lib().llg_amr_allfft_demag(fine_op.h, C.byref(mat), _dp(m), None if mk is None else mk.ctypes.data,
                                       C.byref(g), _dp(bf), _dp(bc)))
     return bf, bc
+
+
+def allfft_demag_device(fine_op, material, m_ptr, mask_ptr, base_grid, b_fine_ptr, b_coarse_ptr, stream_ptr=0):
+    """AllFft demag on device arrays (integers, e.g. torch tensors' data_ptr()): m_fine and
+    b_fine AoS float64 [ny*nx][3] of the fine grid, b_coarse of the base grid, mask uint8 or 0;
+    asynchronous on the stream."""
+    mc = material._c()
+    bg = base_grid._c()
+    _check(lib().llg_amr_allfft_demag_device(fine_op.h, C.byref(mc), m_ptr, mask_ptr or None, C.byref(bg),
+                                             b_fine_ptr, b_coarse_ptr, stream_ptr or None))
 
 
 # ------------------------------------------------------------------ OVF 2.0 (ovf.rs)

@@ -120,3 +120,30 @@ def test_allfft_matches_oracle(gpu, orc):
     # a periodic operator is refused (the AllFft demag uses open boundaries)
     with pytest.raises(gpu.LLGError):
         gpu.allfft_demag(gpu.DemagOp(fine_g, pbc_x=2), gm, m, mask, base_g)
+
+
+def test_allfft_device_entry_equals_host_entry(gpu):
+    """llg_amr_allfft_demag_device on resident arrays gives the host entry's bits."""
+    import torch
+
+    import workloads as W
+
+    nx = ny = 48
+    mf = W.amr_fine_vortex(4 * nx, 4 * ny, 4e-9 / 4, 4e-9 / 4)
+    fg = gpu.Grid2D(4 * nx, 4 * ny, 1e-9, 1e-9, 3e-9)
+    bg = gpu.Grid2D(nx, ny, 4e-9, 4e-9, 3e-9)
+    mat = gpu.Material(8e5, 1.3e-11, demag=True)
+    op = gpu.DemagOp(fg)
+    mask = np.ones(fg.nx * fg.ny, dtype=np.uint8)
+    mask[: fg.nx * 5] = 0
+    bf, bc = gpu.allfft_demag(op, mat, mf, mask, bg)
+    d_m = torch.from_numpy(np.ascontiguousarray(mf)).cuda()
+    d_k = torch.from_numpy(mask).cuda()
+    d_bf = torch.empty_like(d_m)
+    d_bc = torch.empty((nx * ny, 3), dtype=torch.float64, device="cuda")
+    gpu.allfft_demag_device(op, mat, d_m.data_ptr(), d_k.data_ptr(), bg, d_bf.data_ptr(), d_bc.data_ptr(),
+                            torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_bf.cpu().numpy(), bf)
+    assert np.array_equal(d_bc.cpu().numpy(), bc)
+    op.close()
