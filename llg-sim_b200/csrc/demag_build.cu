@@ -226,6 +226,31 @@ __global__ void k_fft_strided(cx<R>* data, FftPlan plan, const cx<R>* tw2, long 
     for (int t = threadIdx.x; t < plan.L; t += blockDim.x) data[base + t * elem_stride] = res[t];
 }
 
+// Column transforms of adjacent signals (stride between signals 1 element): a block
+// takes NS neighbouring columns, so that one row of the tile is NS consecutive
+// elements in memory (whole 32-byte sectors in FP64 instead of half ones); each
+// signal's arithmetic is the one of k_fft_strided.
+template <typename R>
+__global__ void k_fft_strided_tiled(cx<R>* data, FftPlan plan, const cx<R>* tw2, long long elem_stride, int nsig_a,
+                                    long long stride_b, int ns, int inverse) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int L = plan.L;
+    cx<R>* A = reinterpret_cast<cx<R>*>(smem_raw);
+    cx<R>* B = A + (size_t)ns * L;
+    const int tiles_a = nsig_a / ns;
+    const long long base = (long long)(blockIdx.x % tiles_a) * ns + (long long)(blockIdx.x / tiles_a) * stride_b;
+    for (int e = threadIdx.x; e < ns * L; e += blockDim.x) {
+        const int c = e % ns, t = e / ns;
+        A[(size_t)c * L + t] = data[base + c + t * elem_stride];
+    }
+    __syncthreads();
+    cx<R>* res = fft_smem<R>(A, B, ns, plan, tw2, inverse != 0);
+    for (int e = threadIdx.x; e < ns * L; e += blockDim.x) {
+        const int c = e % ns, t = e / ns;
+        data[base + c + t * elem_stride] = res[(size_t)c * L + t];
+    }
+}
+
 template __global__ void k_twiddles<float>(cx<float>*, int);
 template __global__ void k_twiddles<double>(cx<double>*, int);
 
@@ -312,6 +337,21 @@ template <typename R>
 cudaError_t launch_fft_strided(void* data, int L, const void* tw2, long long elem_stride, int nsig_a, long long stride_a,
                                int nsig_b, long long stride_b, bool inverse, cudaStream_t s) {
     FftPlan plan = make_plan(L);
+    if (elem_stride > 1 && stride_a == 1) {
+        // adjacent columns: tile NS of them per block where shared memory allows
+        int ns = 1;
+        while (ns < 8 && nsig_a % (2 * ns) == 0 && 2 * (size_t)(2 * ns) * L * sizeof(cx<R>) <= 200 * 1024) ns *= 2;
+        if (ns > 1) {
+            const size_t smem = 2 * (size_t)ns * L * sizeof(cx<R>);
+            cudaError_t e = cudaFuncSetAttribute(k_fft_strided_tiled<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+            k_fft_strided_tiled<R><<<(nsig_a / ns) * nsig_b, 256, smem, s>>>(
+                reinterpret_cast<cx<R>*>(data), plan, reinterpret_cast<const cx<R>*>(tw2), elem_stride, nsig_a,
+                stride_b, ns, inverse ? 1 : 0);
+            return cudaGetLastError();
+        }
+    }
     size_t smem = 2 * (size_t)L * sizeof(cx<R>);
     cudaError_t e = cudaFuncSetAttribute(k_fft_strided<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
