@@ -1,7 +1,8 @@
-"""The fused row pass (end of RK stage s + start of stage s+1 in one kernel) and
-the column pass without staging must give exactly the bits of the unfused,
-staged passes: same operations in the same order.  LLG_B200_NO_FUSE=1 and
-LLG_B200_COL_STAGED=1 select the unfused / staged kernels at solver creation."""
+"""The fused row pass (end of RK stage s + start of stage s+1 in one kernel) must
+give exactly the bits of the unfused passes: same operations in the same order.
+LLG_B200_NO_FUSE=1 selects the unfused kernels at solver creation; the column
+form (staged or lean tables) is fixed by LLG_B200_COLUMN_FORM and must not change
+the bits either."""
 import numpy as np
 import pytest
 
@@ -33,7 +34,7 @@ def _pair(gpu, monkeypatch, c, prec, env):
 def test_fused_rk45_equals_unfused(orc, gpu, monkeypatch, nx, ny, dmi, ku, masked, prec):
     msk = holes_mask(nx, ny, [(nx // 5, ny // 6, max(3, ny // 5))]) if masked else None
     c = case(nx, ny, dx=2e-9, dy=2e-9, dz=2e-9, ms=5.8e5, a_ex=1.5e-11, k_u=ku, dmi=dmi, mask=msk)
-    fused, plain = _pair(gpu, monkeypatch, c, prec, ["LLG_B200_NO_FUSE", "LLG_B200_COL_STAGED"])
+    fused, plain = _pair(gpu, monkeypatch, c, prec, ["LLG_B200_NO_FUSE"])
     m = random_m(orc, nx * ny, 31 + nx, msk)
     fused.set_state(m)
     plain.set_state(m)
@@ -67,14 +68,28 @@ def test_fused_rk23_relax_equals_unfused(orc, gpu, monkeypatch, prec):
     assert np.array_equal(fused.get_state(), plain.get_state())
 
 
-def test_direct_column_equals_staged(orc, gpu, monkeypatch):
+def test_fused_with_lean_column_equals_unfused_staged(orc, gpu, monkeypatch):
+    """Fused rows + lean column (form 1) against unfused rows + staged column (form 0)."""
     nx, ny = 512, 1024
     c = case(nx, ny, dmi=2e-3)
-    direct, staged = _pair(gpu, monkeypatch, c, 0, ["LLG_B200_COL_STAGED"])
+    monkeypatch.setenv("LLG_B200_COLUMN_FORM", "1")
+    lean = gpu_solver(gpu, c, 0)
+    monkeypatch.setenv("LLG_B200_COLUMN_FORM", "0")
+    monkeypatch.setenv("LLG_B200_NO_FUSE", "1")
+    staged = gpu_solver(gpu, c, 0)
+    monkeypatch.delenv("LLG_B200_COLUMN_FORM")
+    monkeypatch.delenv("LLG_B200_NO_FUSE")
+    assert lean.fft_plans()[1] == 1 and staged.fft_plans()[1] == 0
     m = random_m(orc, nx * ny, 77)
-    direct.set_state(m)
+    lean.set_state(m)
     staged.set_state(m)
-    assert np.array_equal(direct.compute_demag_field(), staged.compute_demag_field())
+    assert np.array_equal(lean.compute_demag_field(), staged.compute_demag_field())
+    p1 = gpu.LLGParams(GAMMA, 0.3, 1e-14, (0.01, 0.0, 0.02))
+    p2 = gpu.LLGParams(GAMMA, 0.3, 1e-14, (0.01, 0.0, 0.02))
+    a = lean.run_rk45(p1, 2, 1e-5, 0.8, 1e-19, 1e-11, n_accepted=4)
+    b = staged.run_rk45(p2, 2, 1e-5, 0.8, 1e-19, 1e-11, n_accepted=4)
+    assert a[:2] == b[:2]
+    assert np.array_equal(lean.get_state(), staged.get_state())
 
 
 @pytest.mark.parametrize("prec", [0, 1])
