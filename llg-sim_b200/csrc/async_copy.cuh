@@ -75,6 +75,19 @@ struct alignas(16) Vec16 {
     static constexpr int W = 16 / (int)sizeof(R);
     R v[W];
 };
+// W consecutive reals loaded / stored as one vector (W * sizeof(R) bytes, aligned).
+template <typename R, int W>
+struct alignas(sizeof(R) * W) VecW {
+    R v[W];
+};
+template <typename R, int W>
+__device__ __forceinline__ VecW<R, W> ldw(const R* p) {
+    return *reinterpret_cast<const VecW<R, W>*>(p);
+}
+template <typename R, int W>
+__device__ __forceinline__ void stw(R* p, const VecW<R, W>& x) {
+    *reinterpret_cast<VecW<R, W>*>(p) = x;
+}
 template <typename R>
 __device__ __forceinline__ Vec16<R> ldv(const R* p) {
     return *reinterpret_cast<const Vec16<R>*>(p);

@@ -12,6 +12,19 @@ namespace llg {
 
 // Row passes: T rows per block; signals: T packed xy rows and T/2 packed z
 // row pairs, each as an even-bin and an odd-bin transform (s = 2g + parity).
+// Registers per thread that let `blocks` blocks of `threads` threads reside on
+// one SM.  The register file is split over the SM's four sub-partitions (16384
+// 32-bit registers each) and a warp takes its registers from the sub-partition it
+// is scheduled on, so the sub-partition with the most warps sets the bound: 112
+// registers allow two 192-thread blocks, not three (18 warps put five on one
+// sub-partition; 96 registers are needed).
+constexpr int regs_for_blocks(int threads, int blocks) {
+    const int warps = blocks * ((threads + 31) / 32);
+    const int per_partition = (warps + 3) / 4;
+    const int r = (16384 / (32 * per_partition)) / 8 * 8;
+    return r > 255 ? 255 : r;
+}
+
 template <typename R, int L, int V = 0>
 struct RowCfg {
     using P = FPlan<R, L, V>;
@@ -20,13 +33,16 @@ struct RowCfg {
     static constexpr int NGRP = T + T / 2;
     static constexpr int NSIG = 2 * NGRP;
     static constexpr int THREADS = NSIG * G;
-    // register caps: one resident block at least (REGCAP), three resident
-    // 192-thread blocks per SM for the FP32 forward and lean inverse passes (MAXREG)
-    static constexpr int REGCAP = (65536 / THREADS) / 8 * 8 > 255 ? 255 : (65536 / THREADS) / 8 * 8;
-    // plan 1 (half the registers per thread) is capped for two resident blocks
-    static constexpr int MAXREG = V == 1 ? ((65536 / (2 * THREADS)) / 8 * 8 > REGCAP ? REGCAP
-                                                                                     : (65536 / (2 * THREADS)) / 8 * 8)
-                                         : (sizeof(R) == 4 && THREADS <= 192) ? 112 : REGCAP;
+    // register caps (regs_for_blocks): one resident block at least (REGCAP); the
+    // FP32 forward and lean inverse passes of 192-thread blocks capped for three
+    // resident blocks, plan 1 (half the registers per thread) for two (MAXREG);
+    // the fused pass of 192-thread blocks for two (FUSEDREG: it holds a transform
+    // and a stencil at once, and the smaller cap only spilled without adding a block)
+    static constexpr int REGCAP = regs_for_blocks(THREADS, 1);
+    static constexpr int MAXREG = V == 1 ? regs_for_blocks(THREADS, 2)
+                                         : (sizeof(R) == 4 && THREADS <= 192) ? regs_for_blocks(THREADS, 3) : REGCAP;
+    static constexpr int FUSEDREG = V == 1 ? regs_for_blocks(THREADS, 2)
+                                           : (sizeof(R) == 4 && THREADS <= 192) ? regs_for_blocks(THREADS, 2) : REGCAP;
     static constexpr int BUF = Pad<R, L, V>::size;
     static constexpr int SMEM_CX = NSIG * BUF + TwTab<R, L, V>::size + L;
     static constexpr size_t SMEM = sizeof(cx<R>) * (size_t)SMEM_CX;
@@ -54,7 +70,12 @@ struct ColCfg {
     static constexpr size_t OFF_XST = al16(OFF_PRE + (LEAN ? 0 : sizeof(cx<R>) * (size_t)L));
     static constexpr size_t OFF_KST = al16(OFF_XST + sizeof(cx<R>) * 3 * (size_t)NC * L);
     static constexpr size_t SMEM = al16(OFF_KST + (LEAN ? 0 : sizeof(r4<R>) * (size_t)NC * (L + 1)));
-    static constexpr int MINB = V == 1 ? 2 : 1;   // plan 1: registers capped for two resident blocks
+    // register cap: plan 1 (half the registers per thread) for two resident blocks,
+    // the lean FP32 form of 192-thread blocks for three (its shared memory allows
+    // three), one block otherwise
+    static constexpr int MAXREG = V == 1 ? regs_for_blocks(THREADS, 2)
+                                         : (LEAN && sizeof(R) == 4 && THREADS <= 192) ? regs_for_blocks(THREADS, 3)
+                                                                                      : regs_for_blocks(THREADS, 1);
 };
 
 template <typename R>
@@ -268,7 +289,7 @@ __device__ __forceinline__ void col_issue_k(const FilmDev* __restrict__ films, c
 }
 
 template <typename R, int L, int V, bool LEAN>
-__global__ void __launch_bounds__(ColCfg<R, L, V, LEAN>::THREADS, ColCfg<R, L, V, LEAN>::MINB) k_column_fast(
+__global__ void __launch_bounds__(ColCfg<R, L, V, LEAN>::THREADS) __maxnreg__((ColCfg<R, L, V, LEAN>::MAXREG)) k_column_fast(
     const FilmDev* __restrict__ films, const WorkItem* __restrict__ items, int nitems, EvalSpec spec) {
     using C = ColCfg<R, L, V, LEAN>;
     using FF = GroupFFT<R, L, false, V>;

@@ -146,6 +146,56 @@ __device__ __forceinline__ bool coef_inside(const LocalCoef<R>& c, int idx) {
     return c.mask == nullptr || c.mask[idx] != 0;
 }
 
+// Rounded operations that the compiler may not fuse or reorder: the cores below
+// spell out every product, sum and fused multiply-add, so a cell's field has the
+// same bits whichever kernel (and whichever surrounding code) evaluates it.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// Arithmetic of the exchange (exchange.rs:45-222), anisotropy (anisotropy.rs:10-26)
+// and DMI (dmi.rs:67-209) terms of one cell from its four neighbour values (real
+// neighbours or ghosts, chosen by the caller); xs / ys: the film has more than one
+// cell along x / y.  Both local-field paths below call these, so a cell gets the
+// same bits from either.
+template <typename R>
+__device__ __forceinline__ void exch_core(const LocalCoef<R>& k, bool xs, bool ys, const R* mc, const R* mim,
+                                          const R* mip, const R* mjm, const R* mjp, R* b) {
+    const R coeff = k.exch, ix2 = k.ix2, iy2 = k.iy2;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        // (m(i+1) - 2 m(i) + m(i-1)) / dx^2 + (...) / dy^2
+        const R d2x = xs ? mul_rn(add_rn(fma_rn((R)-2, mc[c], mip[c]), mim[c]), ix2) : (R)0;
+        const R d2y = ys ? mul_rn(add_rn(fma_rn((R)-2, mc[c], mjp[c]), mjm[c]), iy2) : (R)0;
+        b[c] = fma_rn(coeff, add_rn(d2x, d2y), b[c]);
+    }
+}
+template <typename R>
+__device__ __forceinline__ void anis_core(const LocalCoef<R>& k, const R* mc, R* b) {
+    const R mdotu = fma_rn(mc[2], k.u2, fma_rn(mc[1], k.u1, mul_rn(mc[0], k.u0)));
+    const R f = mul_rn(k.anis, mdotu);
+    b[0] = fma_rn(f, k.u0, b[0]);
+    b[1] = fma_rn(f, k.u1, b[1]);
+    b[2] = fma_rn(f, k.u2, b[2]);
+}
+template <typename R>
+__device__ __forceinline__ void dmi_core(const LocalCoef<R>& k, bool xs, bool ys, const R* mim, const R* mip,
+                                         const R* mjm, const R* mjp, R* b) {
+    const R pref = k.dmi_pref, hx = k.hx, hy = k.hy;
+    const R dmz_dx = xs ? mul_rn(sub_rn(mip[2], mim[2]), hx) : (R)0;
+    const R dmz_dy = ys ? mul_rn(sub_rn(mjp[2], mjm[2]), hy) : (R)0;
+    const R dmx_dx = xs ? mul_rn(sub_rn(mip[0], mim[0]), hx) : (R)0;
+    const R dmy_dy = ys ? mul_rn(sub_rn(mjp[1], mjm[1]), hy) : (R)0;
+    b[0] = fma_rn(pref, dmz_dx, b[0]);
+    b[1] = fma_rn(pref, dmz_dy, b[1]);
+    b[2] = fma_rn(-pref, add_rn(dmx_dx, dmy_dy), b[2]);
+}
+
 // Local effective-field terms at cell (i, j): Zeeman (zeeman.rs:6-12), exchange
 // (exchange.rs:45-222), anisotropy (anisotropy.rs:10-26), DMI (dmi.rs:67-209),
 // accumulated in that order.  With a geometry mask this is the _geom variant
@@ -178,7 +228,7 @@ __device__ __forceinline__ void local_field_c(const LocalCoef<R>& k, NB&& nb, in
     }
     const R dx = k.dx, dy = k.dy, eta = k.eta;
     if (want_ex) {
-        // exchange.rs:45-222 with the ghosts of :8-36
+        // exchange ghosts: exchange.rs:8-36
         const bool he = k.has_eta;
         R mim[3], mip[3], mjm[3], mjp[3];
         if (nx == 1) { cp3(mc, mim); cp3(mc, mip); }
@@ -191,24 +241,11 @@ __device__ __forceinline__ void local_field_c(const LocalCoef<R>& k, NB&& nb, in
             if (vjm) cp3(rjm, mjm); else if (he) ghost_y(mc, (R)-1, eta, dy, mjm); else cp3(mc, mjm);
             if (vjp) cp3(rjp, mjp); else if (he) ghost_y(mc, (R)1, eta, dy, mjp); else cp3(mc, mjp);
         }
-        const R coeff = k.exch, ix2 = k.ix2, iy2 = k.iy2;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            R d2x = nx > 1 ? (mip[c] - (R)2 * mc[c] + mim[c]) * ix2 : (R)0;
-            R d2y = ny > 1 ? (mjp[c] - (R)2 * mc[c] + mjm[c]) * iy2 : (R)0;
-            b[c] += coeff * (d2x + d2y);
-        }
+        exch_core<R>(k, nx > 1, ny > 1, mc, mim, mip, mjm, mjp, b);
     }
-    if (k.anis_on) {
-        // anisotropy.rs:10-26
-        const R coeff = k.anis;
-        R mdotu = mc[0] * k.u0 + mc[1] * k.u1 + mc[2] * k.u2;
-        b[0] += coeff * mdotu * k.u0;
-        b[1] += coeff * mdotu * k.u1;
-        b[2] += coeff * mdotu * k.u2;
-    }
+    if (k.anis_on) anis_core<R>(k, mc, b);
     if (want_dmi) {
-        // dmi.rs:67-209 with the ghosts of :19-52
+        // DMI ghosts: dmi.rs:19-52
         R mim[3], mip[3], mjm[3], mjp[3];
         if (nx == 1) { cp3(mc, mim); cp3(mc, mip); }
         else {
@@ -220,15 +257,26 @@ __device__ __forceinline__ void local_field_c(const LocalCoef<R>& k, NB&& nb, in
             if (j == 0) ghost_y(mc, (R)-1, eta, dy, mjm); else if (vjm) cp3(rjm, mjm); else cp3(mc, mjm);
             if (j == ny - 1) ghost_y(mc, (R)1, eta, dy, mjp); else if (vjp) cp3(rjp, mjp); else cp3(mc, mjp);
         }
-        const R pref = k.dmi_pref, hx = k.hx, hy = k.hy;
-        R dmz_dx = nx > 1 ? (mip[2] - mim[2]) * hx : (R)0;
-        R dmz_dy = ny > 1 ? (mjp[2] - mjm[2]) * hy : (R)0;
-        R dmx_dx = nx > 1 ? (mip[0] - mim[0]) * hx : (R)0;
-        R dmy_dy = ny > 1 ? (mjp[1] - mjm[1]) * hy : (R)0;
-        b[0] += pref * dmz_dx;
-        b[1] += pref * dmz_dy;
-        b[2] += -pref * (dmx_dx + dmy_dy);
+        dmi_core<R>(k, nx > 1, ny > 1, mim, mip, mjm, mjp, b);
     }
+}
+
+// The same terms for a cell whose four neighbours are film cells (not on an edge,
+// no vacuum next to it, film without a mask): no ghost can occur, exchange and DMI
+// read the neighbours themselves.  Same arithmetic as local_field_c.
+template <typename R, typename NB>
+__device__ __forceinline__ void local_field_interior(const LocalCoef<R>& k, NB&& nb, const R* mc, R* b) {
+    b[0] = (R)0 + k.bx;
+    b[1] = (R)0 + k.by;
+    b[2] = (R)0 + k.bz;
+    R rim[3], rip[3], rjm[3], rjp[3];
+    nb(0, rim);
+    nb(1, rip);
+    nb(2, rjm);
+    nb(3, rjp);
+    if (k.ex_on) exch_core<R>(k, true, true, mc, rim, rip, rjm, rjp, b);
+    if (k.anis_on) anis_core<R>(k, mc, b);
+    if (k.dmi_on) dmi_core<R>(k, true, true, rim, rip, rjm, rjp, b);
 }
 
 template <typename R, typename NB>

@@ -5,7 +5,8 @@
 //   1. the inverse x transform of the block's spectrum rows (the last third of
 //      stage s's field evaluation, as k_row_inverse_fast),
 //   2. per cell: the local terms (Zeeman, exchange, anisotropy, DMI in the
-//      reference's order) plus the demag field, the torque k_s (llg_rhs /
+//      reference's order; cells away from edges and vacuum by the ghost-free
+//      path with the same arithmetic) plus the demag field, the torque k_s (llg_rhs /
 //      llg_rhs_relax, llg.rs:20-50), stored for the later combinations and the
 //      error norm, and at once the stage s+1 state
 //        m_{s+1} = normalize(m0 + sum_q dt*a_q k_q)   (llg.rs:869-942 / 296-309)
@@ -41,13 +42,20 @@ __device__ __forceinline__ void torque_cell(const R* mc, const R* b, R pref, R c
 // (forward half: m_in receives m_{s+1}, the combination kidx / a with
 // sf.kidx[sf.nterm - 1] == si.k_out).  Both carry the same request gate.
 template <typename R, int L, int V>
-__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<R, L, V>::MAXREG)) k_row_fused(
+__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<R, L, V>::FUSEDREG)) k_row_fused(
     const FilmDev* __restrict__ films, const WorkItem* __restrict__ items, int nitems, EvalSpec si, EvalSpec sf) {
     using C = RowCfg<R, L, V>;
     using FF = GroupFFT<R, L, false, V>;
     using FI = GroupFFT<R, L, true, V>;
     constexpr int G = C::G, E = C::E, T = C::T, BUF = C::BUF;
-    constexpr int W = Vec16<R>::W, NV = T * L / W;
+    // phase 2 takes W = 2 cells per step of its loop: the stencil (and, with EARLY,
+    // m0 and the previous torques) of both cells are loaded before any arithmetic
+    constexpr int W = 2, NV = T * L / W;
+    using VW = VecW<R, W>;
+    // the early loads of the combination's torques and the ghost-free path of
+    // interior cells need the registers of the FP32 plan-0 budget; the other
+    // instantiations load the torques where they are used and take the general path
+    constexpr bool EARLY = sizeof(R) == 4 && V == 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R>* buf = reinterpret_cast<cx<R>*>(smem_raw);
     cx<R>* twp = buf + C::NSIG * BUF;
@@ -131,7 +139,7 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<
             }
             __syncthreads();
         }
-        // ---- 2. torque of stage s and state of stage s+1, W cells per vector ----
+        // ---- 2. torque of stage s and state of stage s+1, W cells per step ----
         {
             const R* __restrict__ msb = mbuf<R>(F, si.m_in, cur);
             const R* __restrict__ m0 = mbuf<R>(F, MB_M0, cur);
@@ -164,18 +172,29 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<
                     continue;
                 }
                 const int base = j * L + i0;
-                // stencil of m_s: centre, the rows below / above, one x halo on each side
-                Vec16<R> cen[3], dn[3], upv[3];
+                // stencil of m_s: centre, the rows below / above, one x halo on each side;
+                // m0 and the torques of the combination
+                VW cen[3], dn[3], upv[3], a[3], kq[EARLY ? 5 : 1][3];
                 R hl[3], hr[3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    cen[c] = ldv(msb + c * n + base);
-                    if (j > 0) dn[c] = ldv(msb + c * n + base - L);
-                    if (j + 1 < ny) upv[c] = ldv(msb + c * n + base + L);
+                    cen[c] = ldw<R, W>(msb + c * n + base);
+                    if (j > 0) dn[c] = ldw<R, W>(msb + c * n + base - L);
+                    if (j + 1 < ny) upv[c] = ldw<R, W>(msb + c * n + base + L);
                     hl[c] = i0 > 0 ? msb[c * n + base - 1] : (R)0;
                     hr[c] = i0 + W < L ? msb[c * n + base + W] : (R)0;
                 }
-                Vec16<R> ko[3];
+                if constexpr (EARLY) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) a[c] = ldw<R, W>(m0 + c * n + base);
+#pragma unroll
+                    for (int q = 0; q < 5; ++q)
+                        if (q < nq)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) kq[q][c] = ldw<R, W>(kp[q] + c * n + base);
+                }
+                const bool inner = EARLY && cf.mask == nullptr && j > 0 && j + 1 < ny && i0 > 0 && i0 + W < L;
+                VW ko[3];
 #pragma unroll
                 for (int l = 0; l < W; ++l) {
                     const int i = i0 + l;
@@ -190,7 +209,8 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<
                         }
                     };
                     R b[3];
-                    local_field_c<R>(cf, nb, i, j, mc, b);
+                    if (inner) local_field_interior<R>(cf, nb, mc, b);
+                    else local_field_c<R>(cf, nb, i, j, mc, b);
                     if (do_fft) {
 #pragma unroll
                         for (int c = 0; c < 3; ++c) b[c] += *slot(c, r, i);
@@ -201,19 +221,20 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<
                     for (int c = 0; c < 3; ++c) ko[c].v[l] = k[c];
                 }
 #pragma unroll
-                for (int c = 0; c < 3; ++c) stv(kout + c * n + base, ko[c]);
+                for (int c = 0; c < 3; ++c) stw<R, W>(kout + c * n + base, ko[c]);
                 // m_{s+1} = normalize(m0 + sum_q dt*a_q k_q), terms in the tableau's order
-                Vec16<R> a[3];
+                if constexpr (!EARLY) {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) a[c] = ldv(m0 + c * n + base);
+                    for (int c = 0; c < 3; ++c) a[c] = ldw<R, W>(m0 + c * n + base);
+                }
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
                     if (q < nq) {
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
-                            const Vec16<R> kq = ldv(kp[q] + c * n + base);
+                            const VW kv = EARLY ? kq[EARLY ? q : 0][c] : ldw<R, W>(kp[q] + c * n + base);
 #pragma unroll
-                            for (int l = 0; l < W; ++l) a[c].v[l] = a[c].v[l] + cq[q] * kq.v[l];
+                            for (int l = 0; l < W; ++l) a[c].v[l] = a[c].v[l] + cq[q] * kv.v[l];
                         }
                     }
                 }
@@ -233,7 +254,7 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<
                     }
                 }
 #pragma unroll
-                for (int c = 0; c < 3; ++c) stv(mnext + c * n + base, a[c]);
+                for (int c = 0; c < 3; ++c) stw<R, W>(mnext + c * n + base, a[c]);
             }
         }
         if (!do_fft) continue;
