@@ -64,16 +64,65 @@ def dist_env():
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons during a timed region.  NVML is read from a
+    thread every 5 ms (read-only queries; a region of a few milliseconds still gets
+    samples, and one sample is taken at start and at stop); without NVML,
+    nvidia-smi is polled every 200 ms."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
         self.path = None
+        self.nvml = None
+        self.thread = None
+
+    def _nvml_sample(self):
+        nv, h = self.nvml
+        try:
+            self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+            mask = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+            for name, bit in self.REASONS:
+                if mask & bit:
+                    self.reasons.add(name)
+        except Exception:
+            pass
 
     def start(self):
+        self.sm, self.reasons, self.smax = [], set(), None
+        try:
+            import threading
+
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = None
+            try:   # the CUDA device's own PCI address (CUDA and NVML number devices differently)
+                import torch
+
+                pr = torch.cuda.get_device_properties(self.dev)
+                h = nv.nvmlDeviceGetHandleByPciBusId(
+                    f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(self.dev)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.nvml = (nv, h)
+            self.stop_flag = threading.Event()
+            self._nvml_sample()
+
+            def loop():
+                while not self.stop_flag.wait(0.005):
+                    self._nvml_sample()
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -85,6 +134,12 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.nvml is not None:
+            self._nvml_sample()
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            return {"sm_mhz": float(np.median(self.sm)) if self.sm else None, "sm_max_mhz": self.smax,
+                    "samples": len(self.sm), "reasons": sorted(self.reasons), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         self.proc.terminate()
@@ -94,7 +149,7 @@ class ClockSampler:
             self.proc.kill()
         self.fh.close()
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _ in self.REASONS]
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
@@ -109,7 +164,7 @@ class ClockSampler:
                     reasons.add(nm)
         os.unlink(self.path)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
-                "reasons": sorted(reasons)}
+                "reasons": sorted(reasons), "source": "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------

@@ -1383,13 +1383,16 @@ struct Engine final : EngineBase {
         long long launched = 0;
         const long long limit = max_attempts > 0 ? max_attempts : (1LL << 40);
         long long round = 32;
+        bool first = true;   // h_states predates set_control: every film is active in the first round
         for (;;) {
             if (n_acc > 0) {
                 round = 32;
                 for (int f = 0; f < nf; ++f)
-                    if (h_states[f].active) round = std::min(round, n_acc - (h_states[f].n_acc - acc0[f]));
+                    if (first || h_states[f].active)
+                        round = std::min(round, n_acc - (h_states[f].n_acc - acc0[f]));
                 round = std::max(round, 1LL);
             }
+            first = false;
             round = std::min(round, limit - launched);
             long long q = 0;
             for (; q + reps <= round; q += reps)
