@@ -45,6 +45,9 @@ struct RowCfg {
                                            : (sizeof(R) == 4 && THREADS <= 192) ? regs_for_blocks(THREADS, 2) : REGCAP;
     static constexpr int BUF = Pad<R, L, V>::size;
     static constexpr int SMEM_CX = NSIG * BUF + TwTab<R, L, V>::size + L;
+    // the staged spectrum (swizzled slots, stage_slot) lives in the signal buffers
+    static constexpr int STAGE_CX = ((3 * (L + 1) * T * (int)sizeof(cx<R>) / 16 + 7) / 8 * 8) * (16 / (int)sizeof(cx<R>));
+    static_assert(STAGE_CX <= NSIG * BUF, "staged spectrum does not fit the signal buffers");
     static constexpr size_t SMEM = sizeof(cx<R>) * (size_t)SMEM_CX;
 };
 
@@ -77,6 +80,23 @@ struct ColCfg {
                                          : (LEAN && sizeof(R) == 4 && THREADS <= 192) ? regs_for_blocks(THREADS, 3)
                                                                                       : regs_for_blocks(THREADS, 1);
 };
+
+// Staged spectrum of a row block, [c][k][r] in 16-byte pieces (PER complex values).
+// With two rows per block a warp of the inverse transform reads every other piece,
+// which put its lanes on a quarter of the shared-memory banks; the piece slot is
+// XOR-swizzled within each group of eight so that the lanes spread over all of
+// them.  The slots of a group stay in the group, so the staging area needs the
+// piece count rounded up to a multiple of eight.
+template <typename R, int T>
+__device__ __forceinline__ int stage_slot(int p) {
+    if constexpr (T == 2) return p ^ ((p >> 3) & (sizeof(R) == 4 ? 1 : 3));
+    else return p;
+}
+template <typename R, int T>
+__device__ __forceinline__ int stage_index(int e) {
+    constexpr int PER = 16 / (int)sizeof(cx<R>);
+    return stage_slot<R, T>(e / PER) * PER + e % PER;
+}
 
 template <typename R>
 __device__ __forceinline__ void load_tables(cx<R>* twp, const cx<R>* __restrict__ gtwp, int ntwp, cx<R>* pre,
@@ -470,18 +490,25 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((MODE ==
             constexpr int PER = 16 / (int)sizeof(cx<R>);
             for (int p = tid; p < 3 * K1 * T / PER; p += C::THREADS) {
                 const int e = p * PER, r = e % T, ck = e / T;
+                cx<R>* dst = stg + stage_slot<R, T>(p) * PER;
                 if (j0 + r < ny) {
-                    cp_async16(stg + e, X + (size_t)ck * ny + j0 + r);
+                    cp_async16(dst, X + (size_t)ck * ny + j0 + r);
                 } else {
 #pragma unroll
-                    for (int q = 0; q < PER; ++q) stg[e + q] = mkc((R)0, (R)0);
+                    for (int q = 0; q < PER; ++q) dst[q] = mkc((R)0, (R)0);
                 }
             }
             cp_async_wait_all();
             __syncthreads();
-            auto xval = [&](int c, int k, int r) -> cx<R> {
-                if (k <= L) return stg[(c * K1 + k) * T + r];
-                return conjc(stg[(c * K1 + (L2 - k)) * T + r]);
+            static_assert(T != 2 || (2 * G * T / PER) % 32 == 0, "swizzle needs 32-piece strides");
+            const int kb = 2 * t + par;
+            auto xval = [&](int c, int rr, int k, int r) -> cx<R> {
+                // k = kb + 2*G*rr: the swizzle of a slot depends only on the bits below
+                // 2*G*T/PER pieces, so the slots of a thread are its slot at rr = 0 plus
+                // a constant per rr (immediate offsets, no per-value swizzle)
+                const int off = 2 * G * rr * T;
+                if (k <= L) return stg[stage_index<R, T>((c * K1 + kb) * T + r) + off];
+                return conjc(stg[stage_index<R, T>((c * K1 + (L2 - kb)) * T + r) - off]);
             };
             cx<R> v[E];
 #pragma unroll
@@ -489,11 +516,11 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((MODE ==
                 const int k = 2 * (t + G * r) + par;
                 cx<R> z;
                 if (g < T) {
-                    const cx<R> bx = xval(0, k, g), by = xval(1, k, g);
+                    const cx<R> bx = xval(0, r, k, g), by = xval(1, r, k, g);
                     z = mkc(bx.re - by.im, bx.im + by.re);
                 } else {
                     const int ra = 2 * (g - T);
-                    const cx<R> za = xval(2, k, ra), zb = xval(2, k, ra + 1);
+                    const cx<R> za = xval(2, r, k, ra), zb = xval(2, r, k, ra + 1);
                     z = mkc(za.re - zb.im, za.im + zb.re);
                 }
                 v[r] = z;

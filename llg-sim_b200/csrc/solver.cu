@@ -760,30 +760,34 @@ struct Engine final : EngineBase {
             c.erase(std::unique(c.begin(), c.end()), c.end());
             return c;
         };
-        // best grid of one pass; *best_ms receives its time (4 launches)
+        // best grid of one pass; *best_ms receives its time (4 launches).  The
+        // candidates are timed in three interleaved sweeps and each keeps its
+        // fastest sweep, so a transient slowdown does not decide the choice.
         auto tune = [&](int which, const EvalSpec& spec, LaunchGeom& geom, int* grid, int items, int occ,
                         float* best_ms) -> int {
-            float best = 1e30f;
-            int best_g = *grid;
             auto one = [&]() {
                 return which == 3 ? launch_fused<R>(spec, next, geom, stream) : launch_one<R>(which, spec, geom, stream);
             };
-            for (int g : candidates(items, occ)) {
-                *grid = g;
-                for (int w = 0; w < 2; ++w) CUDA_TRY(one());
-                CUDA_TRY(cudaEventRecord(e0, stream));
-                for (int r = 0; r < 4; ++r) CUDA_TRY(one());
-                CUDA_TRY(cudaEventRecord(e1, stream));
-                CUDA_TRY(cudaEventSynchronize(e1));
-                float ms = 0.f;
-                CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-                if (ms < best) {
-                    best = ms;
-                    best_g = g;
+            const std::vector<int> cand = candidates(items, occ);
+            std::vector<float> tmin(cand.size(), 1e30f);
+            for (int sweep = 0; sweep < 3; ++sweep) {
+                for (size_t ci = 0; ci < cand.size(); ++ci) {
+                    *grid = cand[ci];
+                    for (int w = 0; w < 2; ++w) CUDA_TRY(one());
+                    CUDA_TRY(cudaEventRecord(e0, stream));
+                    for (int r = 0; r < 4; ++r) CUDA_TRY(one());
+                    CUDA_TRY(cudaEventRecord(e1, stream));
+                    CUDA_TRY(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+                    tmin[ci] = std::min(tmin[ci], ms);
                 }
             }
-            *grid = best_g;
-            *best_ms = best;
+            size_t bi = 0;
+            for (size_t ci = 1; ci < cand.size(); ++ci)
+                if (tmin[ci] < tmin[bi]) bi = ci;
+            *grid = cand[bi];
+            *best_ms = tmin[bi];
             return LLG_OK;
         };
         auto tune_row = [&](size_t i, int v, float* total) -> int {
