@@ -23,10 +23,13 @@ cudaError_t build_demag_kernel_pbc(int nx, int ny, double dx, double dy, double 
                                    void* planes_out, cudaStream_t s);
 // Builds the demag kernel spectrum of an open-boundary nx x ny grid in FP64 on
 // the GPU.  khat_out: (nx+1)*(ny+1) real4 in the solver precision, scaled by
-// 1/(4 nx ny); k64_out_dev: 4*(ny+1)*(nx+1) doubles, unscaled, layout [c][ky][kx].
+// 1/(4 nx ny), one column of ny+1 entries per kx; with split_columns (even ny)
+// each column holds its even ky (0, 2, .., ny) and then its odd ky (1, 3, ..,
+// ny-1), the order in which the register-FFT column pass reads them (khat_index).
+// k64_out_dev: 4*(ny+1)*(nx+1) doubles, unscaled, layout [c][ky][kx].
 // Synchronises the stream.
 cudaError_t build_demag_kernel(int nx, int ny, double dx, double dy, double dz, bool fp64_out, void* khat_out,
-                               double* k64_out_dev, cudaStream_t s);
+                               double* k64_out_dev, cudaStream_t s, bool split_columns = false);
 
 
 // The demag operator of llg_demag_op_create applied to a device AoS FP64 m on

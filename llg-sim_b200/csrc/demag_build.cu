@@ -135,12 +135,13 @@ __global__ void k_kernel_expand(int nx, int ny, const double* __restrict__ quad,
 
 template <typename R>
 __global__ void k_kernel_extract(int nx, int ny, const cx<double>* __restrict__ planes, double scale,
-                                 r4<R>* __restrict__ khat, double* __restrict__ k64) {
+                                 r4<R>* __restrict__ khat, double* __restrict__ k64, bool split) {
     const int px = 2 * nx, py = 2 * ny;
     const long long np = (long long)px * py;
     const int total = (nx + 1) * (ny + 1);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
         const int kx = e / (ny + 1), ky = e % (ny + 1);
+        const int slot = split ? kx * (ny + 1) + khat_index(ky, ny) : e;
         double v[4];
         for (int c = 0; c < 4; ++c) v[c] = planes[c * np + (long long)ky * px + kx].re;
         r4<R> o;
@@ -148,7 +149,7 @@ __global__ void k_kernel_extract(int nx, int ny, const cx<double>* __restrict__ 
         o.y = (R)(v[1] * scale);
         o.z = (R)(v[2] * scale);
         o.w = (R)(v[3] * scale);
-        khat[e] = o;
+        khat[slot] = o;
         // export layout [c][ky][kx]
         for (int c = 0; c < 4; ++c) k64[((long long)c * (ny + 1) + ky) * (nx + 1) + kx] = v[c];
     }
@@ -372,7 +373,8 @@ template cudaError_t launch_fft_strided<double>(void*, int, const void*, long lo
     } while (0)
 
 cudaError_t build_demag_kernel(int nx, int ny, double dx, double dy, double dz, bool fp64_out, void* khat_out,
-                               double* k64_out_dev, cudaStream_t s) {
+                               double* k64_out_dev, cudaStream_t s, bool split_columns) {
+    if (split_columns && (ny % 2) != 0) return cudaErrorInvalidValue;
     const int px = 2 * nx, py = 2 * ny;
     const long long np = (long long)px * py;
     double* quad = nullptr;
@@ -409,11 +411,11 @@ cudaError_t build_demag_kernel(int nx, int ny, double dx, double dy, double dz, 
         const double scale = 1.0 / (double)np;
         int blocks = ((nx + 1) * (ny + 1) + 255) / 256;
         if (fp64_out)
-            k_kernel_extract<double><<<blocks, 256, 0, s>>>(nx, ny, planes, scale,
-                                                            reinterpret_cast<r4<double>*>(khat_out), k64_out_dev);
+            k_kernel_extract<double><<<blocks, 256, 0, s>>>(
+                nx, ny, planes, scale, reinterpret_cast<r4<double>*>(khat_out), k64_out_dev, split_columns);
         else
-            k_kernel_extract<float><<<blocks, 256, 0, s>>>(nx, ny, planes, scale,
-                                                           reinterpret_cast<r4<float>*>(khat_out), k64_out_dev);
+            k_kernel_extract<float><<<blocks, 256, 0, s>>>(
+                nx, ny, planes, scale, reinterpret_cast<r4<float>*>(khat_out), k64_out_dev, split_columns);
         if ((err = cudaGetLastError()) != cudaSuccess) break;
         err = cudaStreamSynchronize(s);
     } while (0);

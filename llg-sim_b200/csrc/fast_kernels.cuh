@@ -405,9 +405,11 @@ __global__ void __launch_bounds__(ColCfg<R, L, V, LEAN>::THREADS) __maxnreg__((C
             for (int r = 0; r < E; ++r) {
                 const int kk = t + G * r;
                 const int ky = 2 * kk + par;
-                // the kernel spectrum is even in ky except Kxy, which is odd
+                // the kernel spectrum is even in ky except Kxy, which is odd; the
+                // column is parity-split (khat_index): ky and L2 - ky have the parity
+                // of this signal, so a warp reads consecutive entries
                 const bool up = ky > ny;
-                const r4<R> K = kc[up ? L2 - ky : ky];
+                const r4<R> K = kc[par ? (up ? ny / 2 + L - kk : ny / 2 + 1 + kk) : (up ? L - kk : kk)];
                 const R kxy = up ? -K.y : K.y;
                 const int pi = padi<E>(kk);
                 cx<R> out;

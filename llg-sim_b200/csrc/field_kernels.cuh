@@ -33,6 +33,14 @@ struct __align__(4 * sizeof(R)) r4 {
     R x, y, z, w;
 };
 
+// Entry of ky (0..ny, ny even) in a parity-split kernel column: the even ky
+// first (ky / 2), then the odd ones (ny / 2 + 1 + (ky - 1) / 2).  A warp of the
+// register-FFT column pass reads bins of one parity at consecutive kk, which are
+// then consecutive entries.
+__host__ __device__ __forceinline__ int khat_index(int ky, int ny) {
+    return (ky & 1) ? ny / 2 + 1 + (ky >> 1) : (ky >> 1);
+}
+
 template <typename R>
 __device__ __forceinline__ R* mbuf(const FilmDev& F, int id, int cur) {
     switch (id) {

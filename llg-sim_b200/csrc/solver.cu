@@ -577,8 +577,9 @@ struct Engine final : EngineBase {
                     if ((rc = dalloc(&kh, sizeof(r4<R>) * (size_t)(nx + 1) * (ny + 1)))) return rc;
                     F.Khat = kh;
                     if ((rc = dalloc(&d_k64[f], sizeof(double) * 4 * (size_t)(nx + 1) * (ny + 1)))) return rc;
+                    // the register-FFT column pass reads parity-split columns
                     CUDA_TRY(build_demag_kernel(nx, ny, g[f].dx, g[f].dy, g[f].dz, sizeof(R) == 8, kh, d_k64[f],
-                                                stream));
+                                                stream, fcol[f] != 0));
                 }
             }
             for (int b = 0; b < F.nblk; ++b) rows_by[frow[f] ? nx : 0].push_back(WorkItem{f, b});
@@ -734,6 +735,7 @@ struct Engine final : EngineBase {
     int autotune_grids(int nsm) {
         const int forced = forced_plan();
         const bool tuning = !env_flag("LLG_B200_NO_AUTOTUNE");
+        const bool tune_log = env_flag("LLG_B200_TUNE_LOG");
         int rc;
         if ((rc = set_control(idle_control(), nullptr, nullptr, true))) return rc;
         EvalSpec stage = base_spec(LLG_FIELD_FULL);
@@ -786,8 +788,22 @@ struct Engine final : EngineBase {
             size_t bi = 0;
             for (size_t ci = 1; ci < cand.size(); ++ci)
                 if (tmin[ci] < tmin[bi]) bi = ci;
+            // candidates are in increasing grid size: take the smallest grid within 2 %
+            // of the fastest (equal in isolation, a pass with fewer resident blocks
+            // measured faster between its neighbours in a step)
+            for (size_t ci = 0; ci < bi; ++ci)
+                if (tmin[ci] <= 1.02f * tmin[bi]) {
+                    bi = ci;
+                    break;
+                }
             *grid = cand[bi];
             *best_ms = tmin[bi];
+            if (tune_log) {   // LLG_B200_TUNE_LOG=1: candidate grids and their times on stderr
+                std::fprintf(stderr, "llg_b200 tune pass %d items %d:", which, items);
+                for (size_t ci = 0; ci < cand.size(); ++ci)
+                    std::fprintf(stderr, " %d=%.4f%s", cand[ci], tmin[ci] / 4, ci == bi ? "*" : "");
+                std::fprintf(stderr, "\n");
+            }
             return LLG_OK;
         };
         auto tune_row = [&](size_t i, int v, float* total) -> int {
