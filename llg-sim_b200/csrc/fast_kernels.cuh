@@ -36,13 +36,14 @@ struct RowCfg {
     // register caps (regs_for_blocks): one resident block at least (REGCAP); the
     // FP32 forward and lean inverse passes of 192-thread blocks capped for three
     // resident blocks, plan 1 (half the registers per thread) for two (MAXREG);
-    // the fused pass of 192-thread blocks for two (FUSEDREG: it holds a transform
-    // and a stencil at once, and the smaller cap only spilled without adding a block)
+    // the fused pass and the inverse passes with an epilogue, 192-thread FP32
+    // blocks, for two (REG2: they hold a transform and a stencil at once; the
+    // smaller cap only spilled without adding a block)
     static constexpr int REGCAP = regs_for_blocks(THREADS, 1);
     static constexpr int MAXREG = V == 1 ? regs_for_blocks(THREADS, 2)
                                          : (sizeof(R) == 4 && THREADS <= 192) ? regs_for_blocks(THREADS, 3) : REGCAP;
-    static constexpr int FUSEDREG = V == 1 ? regs_for_blocks(THREADS, 2)
-                                           : (sizeof(R) == 4 && THREADS <= 192) ? regs_for_blocks(THREADS, 2) : REGCAP;
+    static constexpr int REG2 = V == 1 ? regs_for_blocks(THREADS, 2)
+                                       : (sizeof(R) == 4 && THREADS <= 192) ? regs_for_blocks(THREADS, 2) : REGCAP;
     static constexpr int BUF = Pad<R, L, V>::size;
     static constexpr int SMEM_CX = NSIG * BUF + TwTab<R, L, V>::size + L;
     // the staged spectrum (swizzled slots, stage_slot) lives in the signal buffers
@@ -456,7 +457,7 @@ __global__ void __launch_bounds__(ColCfg<R, L, V, LEAN>::THREADS) __maxnreg__((C
 // MODE 0: full epilogue; 1: no epilogue, the demag field is written to the film's
 // bdem planes for k_stage_torque; 2: the minimiser epilogue (RHS_MINIMIZE).
 template <typename R, int L, int MODE, int V>
-__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((MODE == 1 ? RowCfg<R, L, V>::MAXREG : RowCfg<R, L, V>::REGCAP)) k_row_inverse_fast(const FilmDev* __restrict__ films,
+__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((MODE == 1 ? RowCfg<R, L, V>::MAXREG : RowCfg<R, L, V>::REG2)) k_row_inverse_fast(const FilmDev* __restrict__ films,
                                                                             const WorkItem* __restrict__ items,
                                                                             int nitems, EvalSpec spec) {
     using C = RowCfg<R, L, V>;
@@ -509,6 +510,10 @@ __global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((MODE ==
                 // 2*G*T/PER pieces, so the slots of a thread are its slot at rr = 0 plus
                 // a constant per rr (immediate offsets, no per-value swizzle)
                 const int off = 2 * G * rr * T;
+                if constexpr (T != 2) {   // identity slots
+                    if (k <= L) return stg[(c * K1 + k) * T + r];
+                    return conjc(stg[(c * K1 + (L2 - k)) * T + r]);
+                }
                 if (k <= L) return stg[stage_index<R, T>((c * K1 + kb) * T + r) + off];
                 return conjc(stg[stage_index<R, T>((c * K1 + (L2 - kb)) * T + r) - off]);
             };

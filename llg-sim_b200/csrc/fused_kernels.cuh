@@ -42,7 +42,7 @@ __device__ __forceinline__ void torque_cell(const R* mc, const R* b, R pref, R c
 // (forward half: m_in receives m_{s+1}, the combination kidx / a with
 // sf.kidx[sf.nterm - 1] == si.k_out).  Both carry the same request gate.
 template <typename R, int L, int V>
-__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<R, L, V>::FUSEDREG)) k_row_fused(
+__global__ void __launch_bounds__(RowCfg<R, L, V>::THREADS) __maxnreg__((RowCfg<R, L, V>::REG2)) k_row_fused(
     const FilmDev* __restrict__ films, const WorkItem* __restrict__ items, int nitems, EvalSpec si, EvalSpec sf) {
     using C = RowCfg<R, L, V>;
     using FF = GroupFFT<R, L, false, V>;
