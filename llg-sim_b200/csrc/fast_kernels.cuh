@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(ColCfg<R, L, V, LEAN>::THREADS) __maxnreg__((C
     using FF = GroupFFT<R, L, false, V>;
     using FI = GroupFFT<R, L, true, V>;
     constexpr int G = C::G, E = C::E, BUF = C::BUF, NC = C::NC;
-    constexpr int ny = L, L2 = 2 * L;
+    constexpr int ny = L;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t bars[2];   // 0: spectrum columns, 1: kernel columns
     __shared__ int s_timeout;

@@ -204,6 +204,22 @@ __device__ __forceinline__ void dmi_core(const LocalCoef<R>& k, bool xs, bool ys
     b[2] = fma_rn(-pref, add_rn(dmx_dx, dmy_dy), b[2]);
 }
 
+// Torque of one cell from m and B (llg.rs:20-32 with c1 = 1, c2 = alpha; the
+// damping-only relax torque llg.rs:38-50 with c1 = 0, c2 = 1), with the same
+// explicit rounding in every kernel that forms it.
+template <typename R>
+__device__ __forceinline__ void torque_cell(const R* mc, const R* b, R pref, R c1, R c2, R* k) {
+    const R t0 = fma_rn(mc[1], b[2], -mul_rn(mc[2], b[1]));
+    const R t1 = fma_rn(mc[2], b[0], -mul_rn(mc[0], b[2]));
+    const R t2 = fma_rn(mc[0], b[1], -mul_rn(mc[1], b[0]));
+    const R u0 = fma_rn(mc[1], t2, -mul_rn(mc[2], t1));
+    const R u1 = fma_rn(mc[2], t0, -mul_rn(mc[0], t2));
+    const R u2 = fma_rn(mc[0], t1, -mul_rn(mc[1], t0));
+    k[0] = mul_rn(pref, fma_rn(c2, u0, mul_rn(c1, t0)));
+    k[1] = mul_rn(pref, fma_rn(c2, u1, mul_rn(c1, t1)));
+    k[2] = mul_rn(pref, fma_rn(c2, u2, mul_rn(c1, t2)));
+}
+
 // Local effective-field terms at cell (i, j): Zeeman (zeeman.rs:6-12), exchange
 // (exchange.rs:45-222), anisotropy (anisotropy.rs:10-26), DMI (dmi.rs:67-209),
 // accumulated in that order.  With a geometry mask this is the _geom variant
@@ -594,27 +610,12 @@ __device__ __forceinline__ void row_epilogue(const FilmDev& F, const EvalSpec& s
             if (spec.rhs == RHS_FIELD) {
                 bout[idx] = b[0]; bout[n + idx] = b[1]; bout[2 * n + idx] = b[2];
             }
-            // torque m x B and m x (m x B)
-            R t0 = mc[1] * b[2] - mc[2] * b[1];
-            R t1 = mc[2] * b[0] - mc[0] * b[2];
-            R t2 = mc[0] * b[1] - mc[1] * b[0];
+            // torque m x B and m x (m x B) (llg.rs:20-32, 38-50)
             R k[3] = {(R)0, (R)0, (R)0};
             if (spec.rhs == RHS_LLG || spec.rhs == RHS_RELAX) {
-                R u0 = mc[1] * t2 - mc[2] * t1;
-                R u1 = mc[2] * t0 - mc[0] * t2;
-                R u2 = mc[0] * t1 - mc[1] * t0;
                 const R denom = (R)1 + alp * alp;
-                if (spec.rhs == RHS_LLG) {
-                    const R pref = -gam / denom;  // llg.rs:20-32
-                    k[0] = pref * (t0 + alp * u0);
-                    k[1] = pref * (t1 + alp * u1);
-                    k[2] = pref * (t2 + alp * u2);
-                } else {
-                    const R pref = -gam * alp / denom;  // llg.rs:38-50
-                    k[0] = pref * u0;
-                    k[1] = pref * u1;
-                    k[2] = pref * u2;
-                }
+                const bool llg = spec.rhs == RHS_LLG;
+                torque_cell<R>(mc, b, llg ? -gam / denom : -gam * alp / denom, llg ? (R)1 : (R)0, llg ? alp : (R)1, k);
                 kout[idx] = k[0]; kout[n + idx] = k[1]; kout[2 * n + idx] = k[2];
             }
             if (spec.reduce) {

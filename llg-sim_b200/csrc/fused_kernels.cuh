@@ -23,21 +23,6 @@
 
 namespace llg {
 
-// Torque of one cell from m and B (llg.rs:20-32 with c1 = 1, c2 = alpha; the
-// damping-only relax torque llg.rs:38-50 with c1 = 0, c2 = 1), as k_stage_torque.
-template <typename R>
-__device__ __forceinline__ void torque_cell(const R* mc, const R* b, R pref, R c1, R c2, R* k) {
-    const R t0 = mc[1] * b[2] - mc[2] * b[1];
-    const R t1 = mc[2] * b[0] - mc[0] * b[2];
-    const R t2 = mc[0] * b[1] - mc[1] * b[0];
-    const R u0 = mc[1] * t2 - mc[2] * t1;
-    const R u1 = mc[2] * t0 - mc[0] * t2;
-    const R u2 = mc[0] * t1 - mc[1] * t0;
-    k[0] = pref * (c1 * t0 + c2 * u0);
-    k[1] = pref * (c1 * t1 + c2 * u1);
-    k[2] = pref * (c1 * t2 + c2 * u2);
-}
-
 // si: stage s (inverse half: m_in, k_out, rhs, field terms); sf: stage s+1
 // (forward half: m_in receives m_{s+1}, the combination kidx / a with
 // sf.kidx[sf.nterm - 1] == si.k_out).  Both carry the same request gate.

@@ -53,13 +53,8 @@ __global__ void __launch_bounds__(256, 4) k_stage_torque(const FilmDev* __restri
             const R pref = spec.rhs == RHS_LLG ? -gam / denom : -gam * alp / denom;
             const R c1 = spec.rhs == RHS_LLG ? (R)1 : (R)0;
             const R c2 = spec.rhs == RHS_LLG ? alp : (R)1;
-            const R t0 = mc[1] * b[2] - mc[2] * b[1];
-            const R t1 = mc[2] * b[0] - mc[0] * b[2];
-            const R t2 = mc[0] * b[1] - mc[1] * b[0];
-            const R u0 = mc[1] * t2 - mc[2] * t1;
-            const R u1 = mc[2] * t0 - mc[0] * t2;
-            const R u2 = mc[0] * t1 - mc[1] * t0;
-            const R k[3] = {pref * (c1 * t0 + c2 * u0), pref * (c1 * t1 + c2 * u1), pref * (c1 * t2 + c2 * u2)};
+            R k[3];
+            torque_cell<R>(mc, b, pref, c1, c2, k);
             kout[idx] = k[0];
             kout[n + idx] = k[1];
             kout[2 * n + idx] = k[2];
