@@ -141,7 +141,10 @@ __global__ void k_controller(FilmDev* films, int nfilms, int order, int req) {
         st->n_acc += 1;
         st->t += dt0;
     } else {
-        st->fsal_valid = 0;
+        // RK45: k1 of the unchanged state stays valid (its buffer is not written by
+        // the rejected attempt, and the run / step calls evaluate it before their
+        // first attempt); RK23 re-evaluates it, as the relax loop expects
+        st->fsal_valid = order == 5 ? 1 : 0;
         st->n_rej += 1;
     }
     st->accepted = acc ? 1 : 0;
@@ -1168,15 +1171,25 @@ struct Engine final : EngineBase {
     }
 
     // One integrator attempt; req gates every kernel on StepState::req (relax).
-    int launch_attempt(int kind, int fmask, int req) {
-        int rc;
-        std::vector<EvalSpec> ch;
+    // Stage 1 of an attempt: k1 = f(m0), skipped on the device for films whose
+    // first-same-as-last torque is valid.
+    EvalSpec stage1_spec(int kind, int fmask, int req) {
         EvalSpec e = base_spec(fmask);
         e.req = req;
         e.rhs = kind == KIND_RK45 ? RHS_LLG : RHS_RELAX;
         e.k_out = KB_K1;
         e.skip_if_fsal = 1;
-        ch.push_back(e);
+        return e;
+    }
+
+    // One attempt: stages 1 (unless with_stage1 is false: RK45 graphs, whose
+    // callers evaluate stage 1 once before their first attempt, since after any
+    // attempt k1 of the film's state is valid) to s, then the controller.
+    int launch_attempt(int kind, int fmask, int req, bool with_stage1 = true) {
+        int rc;
+        std::vector<EvalSpec> ch;
+        EvalSpec e = stage1_spec(kind, fmask, req);
+        if (with_stage1) ch.push_back(e);
         e.skip_if_fsal = 0;
         if (kind == KIND_RK45) {
             using namespace dp5;
@@ -1316,7 +1329,8 @@ struct Engine final : EngineBase {
     }
 
     int attempt_graph(int kind, int fmask, int reps, cudaGraphExec_t* out) {
-        return get_graph(graph_key(kind, fmask, reps), reps, [&]() { return launch_attempt(kind, fmask, 0); }, out);
+        return get_graph(graph_key(kind, fmask, reps), reps,
+                         [&]() { return launch_attempt(kind, fmask, 0, kind != KIND_RK45); }, out);
     }
 
     // FSAL validity across calls (llg.rs:854-867, 317-330): same kind, mask and b_ext.
@@ -1351,6 +1365,7 @@ struct Engine final : EngineBase {
         if ((rc = set_control(c, p, inv.get(), false))) return rc;
         cudaGraphExec_t ge = nullptr;
         if ((rc = attempt_graph(kind, fmask, 1, &ge))) return rc;
+        if (kind == KIND_RK45 && (rc = eval(stage1_spec(kind, fmask, 0)))) return rc;
         if ((rc = graph_launch(graph_key(kind, fmask, 1), ge))) return rc;
         if ((rc = read_states())) return rc;
         for (int f = 0; f < nf; ++f) {
@@ -1400,6 +1415,7 @@ struct Engine final : EngineBase {
         const int reps = 8;
         cudaGraphExec_t ge = nullptr, ge1 = nullptr;
         if ((rc = attempt_graph(kind, fmask, reps, &ge))) return rc;
+        if (kind == KIND_RK45 && (rc = eval(stage1_spec(kind, fmask, 0)))) return rc;
         long long launched = 0;
         const long long limit = max_attempts > 0 ? max_attempts : (1LL << 40);
         long long round = 32;
