@@ -440,7 +440,14 @@ def warmstart_leg(L, torch, stream, max_over_ranks, n_films=16, size=256, torque
         tot = max_over_ranks(e0.elapsed_time(e2)) * 1e-3
         en32 = np.array([e.total() for e in b32.compute_energy(bex)])
         en = np.array([e.total() for e in b64.compute_energy(bex)])
-        tq = np.array([r.final_torque_max if r.has_final_torque_max else np.inf for r in r64])
+        # final max |m x B| of every film in FP64 (the relax stops at its step budget
+        # without a final check), after the timed region
+        tq = np.empty(len(fs))
+        for k, f in enumerate(fs):
+            sv = L.Solver(grids[k], mats[k], L.FP64, geom_mask=msk[k])
+            sv.set_state(b64.get_state(k))
+            tq[k] = sv.torque_metric(L.LLGParams(GAMMA, f.alpha, rx["dt0"], f.b_ext), L.FULL, L.TORQUE_MAX)
+            sv.close()
         out = {"wall_s": tot, "fp32_stage_s": t32, "fp64_stage_s": tot - t32,
                "fp32_steps_mean": float(np.mean([r.accepted_steps for r in r32])),
                "fp32_at_cap": int(sum(r.accepted_steps >= max_steps for r in r32)),
@@ -449,17 +456,17 @@ def warmstart_leg(L, torch, stream, max_over_ranks, n_films=16, size=256, torque
                "reached_torque": int((tq <= torque).sum())}
         b32.close()
         b64.close()
-        return out, en, en32, tq
+        return out, en, en32, tq, np.array([r.accepted_steps for r in r32])
 
     all_idx = list(range(n_films))
-    plain, e_plain, e32_plain, t_plain = arm(all_idx, False)
-    learned, e_learn, e32_learn, t_learn = arm(all_idx, True)
+    plain, e_plain, e32_plain, t_plain, s_plain = arm(all_idx, False)
+    learned, e_learn, e32_learn, t_learn, s_learn = arm(all_idx, True)
     rel = np.abs(e_learn - e_plain) / np.abs(e_plain)
     rel32 = np.abs(e32_learn - e32_plain) / np.abs(e32_plain)
     differ = [i for i in all_idx if not rel[i] <= 1e-6]
     fallback = {"films": len(differ), "wall_s": 0.0}
     if differ:
-        fb, _, _, _ = arm(differ, False)
+        fb = arm(differ, False)[0]
         fallback["wall_s"] = fb["wall_s"]
     net.close()
     return {"workload": f"{n_films} films {size}x{size}, 4x4x3 nm, 0-6 holes r 8-24 cells, D U[0,2e-3], 0-30 mT "
@@ -475,7 +482,12 @@ def warmstart_leg(L, torch, stream, max_over_ranks, n_films=16, size=256, torque
             "energy_rel_diff_fp64": {"median": float(np.median(rel)), "max": float(rel.max()),
                                      "learned_lower": int(((e_learn < e_plain) & (rel > 1e-6)).sum()),
                                      "learned_higher": int(((e_learn > e_plain) & (rel > 1e-6)).sum())},
-            "energy_rel_diff_fp32_stage": {"median": float(np.median(rel32)), "max": float(rel32.max())}}
+            "energy_rel_diff_fp32_stage": {"median": float(np.median(rel32)), "max": float(rel32.max())},
+            "films": [{"film": i, "film_cells_frac": round(float(np.mean(films[i].mask != 0)), 3), "b_ext_mT": [round(1e3 * b, 2) for b in films[i].b_ext],
+                       "fp32_steps_plain": int(s_plain[i]), "fp32_steps_learned": int(s_learn[i]),
+                       "final_torque_T_plain": float(t_plain[i]), "final_torque_T_learned": float(t_learn[i]),
+                       "energy_J_plain": float(e_plain[i]), "energy_J_learned": float(e_learn[i]),
+                       "energy_rel_diff": float(rel[i]), "fallback": bool(i in differ)} for i in all_idx]}
 
 
 def amr_leg(L, reps=5):
