@@ -1170,7 +1170,6 @@ struct Engine final : EngineBase {
         return LLG_OK;
     }
 
-    // One integrator attempt; req gates every kernel on StepState::req (relax).
     // Stage 1 of an attempt: k1 = f(m0), skipped on the device for films whose
     // first-same-as-last torque is valid.
     EvalSpec stage1_spec(int kind, int fmask, int req) {
@@ -1182,9 +1181,10 @@ struct Engine final : EngineBase {
         return e;
     }
 
-    // One attempt: stages 1 (unless with_stage1 is false: RK45 graphs, whose
-    // callers evaluate stage 1 once before their first attempt, since after any
-    // attempt k1 of the film's state is valid) to s, then the controller.
+    // One integrator attempt: stages 1 (unless with_stage1 is false: RK45 graphs,
+    // whose callers evaluate stage 1 once before their first attempt, since after
+    // any attempt k1 of the film's state is valid) to s, then the controller; req
+    // gates every kernel on StepState::req (relax).
     int launch_attempt(int kind, int fmask, int req, bool with_stage1 = true) {
         int rc;
         std::vector<EvalSpec> ch;
