@@ -175,7 +175,9 @@ int llg_compute_demag_field(llg_solver* s, double* b_out);
 /* step_llg_rk45_recompute_field_masked_adaptive (llg.rs:795-1026): one attempt
  * on the resident state.  params->dt is read as dt0 and overwritten with the
  * next step size, as the reference mutates LLGParams::dt.  FSAL reuse follows
- * llg.rs:854-867 (valid after an accepted step with the same mask and b_ext). */
+ * llg.rs:854-867 (valid after an accepted step with the same mask and b_ext);
+ * after a rejected attempt the stored k1 of the unchanged state is reused too
+ * instead of being evaluated again (same values: k1 = f(m0) of the same m0). */
 int llg_step_rk45(llg_solver* s, llg_params* params, int32_t field_mask, double max_err, double headroom,
                   double dt_min, double dt_max, double* eps, int32_t* accepted, double* dt_used);
 /* step_llg_rk23_recompute_field_masked_relax_adaptive (llg.rs:278-436). */
