@@ -17,10 +17,12 @@ def test_both_arms_share_the_config_object():
 
 def test_compact_legs_are_short_and_rounded():
     warm = {"workload": "w" * 500, "weights": "x", "plain": {"wall_s": 23.456789, "fp32_stage_s": 10.0},
-            "learned": {"wall_s": 7.123456}, "speedup_total": 3.3333333}
+            "learned": {"wall_s": 7.123456}, "speedup_total": 3.3333333,
+            "films": [{"film": i, "energy_rel_diff": 1e-9, "fallback": False} for i in range(256)]}
     out = bench.compact_legs({"value": 7.123456e8, "ms": 6000.123, "accepted_mean": 1614.2, "rejected": 1},
                              None, warm, None, None, None)
     assert "workload" not in out["warm_start_c5"]
+    assert "films" not in out["warm_start_c5"]   # the per-film table goes to --detail only
     assert out["batch_c3"]["value"] == 7.123e8
     assert len(json.dumps(out)) < 400
 
