@@ -89,12 +89,12 @@ struct ColCfg {
 // them.  The slots of a group stay in the group, so the staging area needs the
 // piece count rounded up to a multiple of eight.
 template <typename R, int T>
-__device__ __forceinline__ int stage_slot(int p) {
+__host__ __device__ __forceinline__ int stage_slot(int p) {
     if constexpr (T == 2) return p ^ ((p >> 3) & (sizeof(R) == 4 ? 1 : 3));
     else return p;
 }
 template <typename R, int T>
-__device__ __forceinline__ int stage_index(int e) {
+__host__ __device__ __forceinline__ int stage_index(int e) {
     constexpr int PER = 16 / (int)sizeof(cx<R>);
     return stage_slot<R, T>(e / PER) * PER + e % PER;
 }
